@@ -1,0 +1,309 @@
+"""Benchmark of the checkerboard Metropolis sweep on B200 (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mclics_b200|reference]
+
+Workload: the GHRL slab of 256 x 256 x 256 sites (x, y periodic, z free), K11:K22:K33 = 1 : 0.5 : 1.5,
+homeotropic anchoring W = 1.5 on both plates, T = 0.8, initial director (0, 0, 1) plus uniform noise of amplitude
+0.1 per component (seed 7), FP32 directors, FP64 reductions. One step = one Monte Carlo sweep of all sites plus its
+measurement (energy, Q tensor, S, acceptance, device-side ang_var adaptation), i.e. one measurement sweep of the
+reference's thermalGPU loop. Metric: site updates per second (whole job, all GPUs).
+
+  value      device time (CUDA events on the engine's stream) of K steps with the lattice resident in HBM. The
+             lattice (211 MB padded) is larger than L2 (126 MB), so no flush is needed between steps.
+  e2e        the same steps through the C ABI as the reference's GPU mode loop drives them, host buffers and
+             host<->device copies inside the timed region: per step the temperature goes up from pinned host
+             memory, the observables record and the whole director field (the reference copies it back after
+             every measurement sweep, src/evolve_thermal.cu:90) come down into pinned host memory.
+  roofline   the sweep kernel(s) only: algorithmic 24 B per site update (one FP32 director read + write) per
+             sweep / kernel time, against the measured HBM copy bandwidth.
+  cpu_baseline  the reference's own OpenMP CPU sweep + measurement (oracle/_ref/mclics_ref_timing, built from the
+             reference sources) on all host cores, on a bounded sample of the same lattice.
+
+--impl reference times that reference CPU path alone (rank 0) and prints its line with "impl": "reference".
+Multi-GPU (torchrun): every rank sweeps its own independent replica of the workload (no data-path collective;
+"scaling": "weak"); value = all ranks' site updates / the slowest rank's device time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NX = NY = NZ = 256
+T = 0.8
+SEED = 7
+BYTES_PER_SITE_UPDATE = 24
+METRIC = "site-updates/s"
+WORKLOAD = "ghrl_slab_256^3_k1:0.5:1.5_homeotropic_W1.5_T0.8"
+
+
+def c2_input_text():
+    return ("Nx %d\nNy %d\nNz %d\ngeometry slab\nxbound periodic\nybound periodic\npotential ghrl\nk11 1\nk22 0.5\n"
+            "k33 1.5\nanchoring_type 0 homeotropic\nW 0 1.5\nanchoring_type 1 homeotropic\nW 1 1.5\nevol thermal\n"
+            "Ti %g\nTf %g\ndT -0.1\nMCT 200\nMCS 1000\nic homogeneous\ntheta_0 0\nphi_0 0\nseed %d\n"
+            % (NX, NY, NZ, T, T, SEED))
+
+
+def c2_initial_state(seed=SEED):
+    """(0, 0, 1) + uniform noise of amplitude 0.1 per component, renormalised (seeded numpy stream)."""
+    rng = np.random.default_rng(seed)
+    n = NX * NY * NZ
+    v = rng.uniform(-0.1, 0.1, size=(n, 3)).astype(np.float32)
+    v[:, 2] += 1.0
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    return v.reshape(-1).astype(np.float32)
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel_key):
+    """Per-launch DRAM traffic of a kernel from the committed ncu summary (profiles/ncu_traffic.json), or None."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    return d.get(kernel_key)
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        def loop():
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                         timeout=5).stdout.strip()
+                    if out:
+                        self.samples.append([x.strip() for x in out.split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+        self._t = threading.Thread(target=loop, daemon=True)
+        self._t.start()
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for k, name in enumerate(names):
+                if len(s) > 5 + k and s[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def reference_cpu(steps, warmup, budget_s=150.0):
+    """Times the reference's own CPU sweep + measurement (oracle/_ref/mclics_ref_timing) on all host cores."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "mclics_ref_timing")
+    if not os.path.exists(exe):
+        return None, "oracle/_ref/mclics_ref_timing not built"
+    import tempfile
+    cores = os.cpu_count() or 1
+    d = tempfile.mkdtemp(prefix="mcl_ref_")
+    with open(os.path.join(d, "c2.txt"), "w") as f:
+        f.write(c2_input_text())
+    env = dict(os.environ, OMP_NUM_THREADS=str(cores))
+
+    def run(w, k):
+        p = subprocess.run([exe, "c2.txt", str(w), str(k), "1", "0.1", str(SEED)], cwd=d, env=env,
+                           capture_output=True, text=True, timeout=900)
+        if p.returncode != 0:
+            raise RuntimeError(p.stderr[-500:])
+        return json.loads(p.stdout.strip().splitlines()[-1])
+
+    # one probe step sizes the sample so that the whole run stays inside the budget
+    probe = run(0, 1)
+    per = max(probe["seconds"], 1e-3)
+    k = max(1, min(steps, int(budget_s / per) - warmup))
+    w = min(warmup, 1)
+    r = run(w, k)
+    r["steps_requested"] = steps
+    return r, None
+
+
+def gpu_arm(args, rank, world, local_rank):
+    import torch
+    import mclics_b200 as M
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    model = M.Model("ghrl", k=(1.0, 0.5, 1.5), surfaces=[("homeotropic", 1.5, 0, 0)] * 2)
+    rep = M.Replica(NX, NY, NZ, "slab", (1, 1, 0), T=T, seed=SEED + 1000 * rank)
+    eng = M.Engine(model, [rep])
+    ni0 = c2_initial_state(SEED + rank)
+    eng.upload(0, ni0)
+    stream = torch.cuda.Stream(device=dev)
+    eng.set_stream(stream.cuda_stream)
+    sites = NX * NY * NZ
+
+    for _ in range(args.warmup):
+        eng.sweeps(1, measure=True)
+    eng.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    eng.profile(True)
+    ms0, n0, l0 = eng.profile_read()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        eng.sweeps(1, measure=True)
+    e1.record(stream)
+    e1.synchronize()
+    clocks.stop()
+    dev_ms = e0.elapsed_time(e1)
+    ms1, n1, l1 = eng.profile_read()
+    eng.profile(False)
+    kernel_ms = (ms1 - ms0) / max(1, n1 - n0)
+    launches = l1 - l0
+    rec = eng.series(0, eng.series_length() - 1, 1)[0]
+
+    # end to end through the C ABI with host buffers
+    host_ni = torch.empty(3 * sites, dtype=torch.float32, pin_memory=True)
+    host_T = torch.tensor([T], dtype=torch.float32, pin_memory=True)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        eng.set_temperature(float(host_T[0]))
+        eng.sweeps(1, measure=True)
+        eng.series(0, eng.series_length() - 1, 1)
+        M.check(M.lib().mcl_download_directors(eng._h, 0, host_ni.data_ptr()))
+    e2e_s = time.perf_counter() - t0
+
+    times = torch.tensor([dev_ms, e2e_s * 1e3], dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(times, op=torch.distributed.ReduceOp.MAX)
+    dev_ms_max, e2e_ms_max = float(times[0]), float(times[1])
+    eng.close()
+    return dict(dev_ms=dev_ms_max, e2e_ms=e2e_ms_max, kernel_ms=kernel_ms, launches=launches, sites=sites,
+                clocks=clocks.summary(), S=float(rec["S"]), E=float(rec["energy"]), acc=float(rec["acceptance"]))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="mclics_b200", choices=["mclics_b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    config = {"workload": WORKLOAD, "lattice": [NX, NY, NZ], "geometry": "slab", "potential": "ghrl",
+              "k11_k22_k33": [1, 0.5, 1.5], "anchoring": "homeotropic W=1.5 (both plates)", "T": T,
+              "step": "1 sweep + measurement", "global_sites_per_step": NX * NY * NZ * max(1, args.gpus),
+              "parallelism": "independent replicas x%d" % max(1, args.gpus),
+              "l2": "inputs larger than L2 (211 MB padded lattice > 126 MB)"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        r, why = reference_cpu(args.steps, args.warmup)
+        if r is None:
+            print(json.dumps({"impl": "reference", "unavailable": why}))
+            return 0
+        v = r["sites"] * r["steps"] / r["seconds"]
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "site-updates/s", "n_gpus": args.gpus,
+                "steps": r["steps"], "warmup": args.warmup, "ms_per_step": 1e3 * r["seconds"] / r["steps"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 accumulators)",
+                "data": "synthetic", "config": config,
+                "cpu_baseline": {"value": v, "unit": "site-updates/s", "cores": r["threads"], "kind": "reference",
+                                 "sample": "%d measured sweeps of the 256^3 lattice after %d warm-up (reference "
+                                           "EvolveN::Monte_Carlo_Step + energy_calculator + Q_tensor + eigen, "
+                                           "GSL replaced by the shim)" % (r["steps"], min(args.warmup, 1))},
+                "e2e": {"value": v, "unit": "site-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    if world > 1:
+        import torch
+        torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    res = gpu_arm(args, rank, world, local_rank)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r, why = reference_cpu(10, 1, budget_s=25.0)
+        if r is not None:
+            cpu = {"value": r["sites"] * r["steps"] / r["seconds"], "unit": "site-updates/s", "cores": r["threads"],
+                   "kind": "reference",
+                   "sample": "%d measured sweeps of the same 256^3 lattice after 1 warm-up, reference OpenMP CPU "
+                             "code (oracle/_ref, GSL shim)" % r["steps"]}
+        else:
+            cpu = {"value": None, "unavailable": why}
+    if world > 1:
+        import torch
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return 0
+    sites_total = res["sites"] * world
+    value = sites_total * args.steps / (res["dev_ms"] / 1e3)
+    e2e = sites_total * args.steps / (res["e2e_ms"] / 1e3)
+    peak, peak_kind = measured_peaks()
+    achieved = res["sites"] * BYTES_PER_SITE_UPDATE / (res["kernel_ms"] / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "site-updates/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": res["dev_ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (f64 accumulators)", "data": "synthetic", "config": config,
+        "e2e": {"value": e2e, "unit": "site-updates/s", "h2d_bytes_per_step": 4,
+                "d2h_bytes_per_step": 144 + 12 * res["sites"]},
+        "gpu_launches": res["launches"],
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "traffic": ncu_traffic("sweep_ghrl_slab_256"),
+                     "kernel_ms_per_sweep": res["kernel_ms"],
+                     "algorithmic_bytes_per_sweep": res["sites"] * BYTES_PER_SITE_UPDATE},
+        "cpu_baseline": cpu,
+        "clocks": res["clocks"],
+        "physics": {"S_last": res["S"], "E_last": res["E"], "acceptance_last": res["acc"]},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,164 @@
+/* mclics_b200 — B200-native checkerboard Metropolis sweep for McLics (C ABI).
+ *
+ * The reference exposes its GPU path as C++ classes: `class EvolveNGPU : public Evolve` with the constructor
+ * (float *ni, int *pt, Parameters *params) (include/evolve.cuh:22-42), the four mode subclasses
+ * {thermal,step,quench,electric}EvolveNGPU (include/evolve.cuh:43-67), selected by name in
+ * src/simulator.cpp:45-53, whose run() loops (src/evolve_{thermal,step,quench,electric}.cu) call
+ * Monte_Carlo_Step_GPU (src/evolve.cu:317-440) and energy_calculator_GPU (src/evolve.cu:442-478). This header
+ * is the plain-C replacement for that boundary: POD structs instead of Parameters (include/parameters.h:18-98),
+ * an opaque engine handle instead of the class with function-local statics (so many simulations, and batches of
+ * replicas, live in one process), and an int status on every call instead of printf + exit(20).
+ *
+ * Every function returns MCL_OK (0) or an MCL_ERR_* code; mcl_last_error() gives the message of the last failure
+ * on the calling thread. No function exits the process or throws. All director arrays crossing this boundary use
+ * the reference layout: 3 floats per site, site (i, j, k) at index i + Nx (j + Ny k) (include/define.h:9-19). */
+#ifndef MCLICS_B200_H_
+#define MCLICS_B200_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MCL_MAX_SURFACES 16
+
+enum mcl_status {
+  MCL_OK = 0,
+  MCL_ERR_ARG = 1,         /* invalid argument (sizes, indices, null pointers, unsupported combination) */
+  MCL_ERR_CUDA = 2,        /* a CUDA call failed (message has the CUDA error string) */
+  MCL_ERR_NOMEM = 3,       /* device or host allocation failed */
+  MCL_ERR_STATE = 4,       /* call not valid in the engine's current state */
+  MCL_ERR_INPUT = 5,       /* input file or parameter error (same checks as src/io.cpp:381-475) */
+  MCL_ERR_IO = 6,          /* file could not be read or written */
+  MCL_ERR_NONFINITE = 7,   /* a director uploaded or produced is NaN/Inf or has zero length */
+  MCL_ERR_NO_DEVICE = 8    /* no CUDA device, or not an sm_100 device */
+};
+
+/* Pair potential (src/potential.cpp:19-56, selected in src/simulator.cpp:234-250). */
+enum mcl_potential { MCL_POT_LL = 0, MCL_POT_GHRL = 1, MCL_POT_PEAR = 2 };
+/* Geometry (src/geometry_{bulk,slab,sphere,custom}.cpp). bulk and slab are analytic on the device (no
+ * point-type array); sphere and custom take pt and normals through mcl_set_geometry. */
+enum mcl_geometry { MCL_GEOM_BULK = 0, MCL_GEOM_SLAB = 1, MCL_GEOM_SPHERE = 2, MCL_GEOM_CUSTOM = 3 };
+/* Surface anchoring (src/anchoring_*.cpp, names in src/geometry.cpp:78-107). */
+enum mcl_anchoring {
+  MCL_ANCH_HOMEOTROPIC = 0,
+  MCL_ANCH_RP = 1,
+  MCL_ANCH_RP_TANGENT = 2,
+  MCL_ANCH_FG = 3,
+  MCL_ANCH_HOMEOTROPIC_GHRL = 4,
+  MCL_ANCH_RP_GHRL = 5,
+  MCL_ANCH_FG_GHRL = 6
+};
+/* Update order within a sweep.
+ *  MCL_SCHED_REF8      the reference CPU's 8 sublattices by parity of (i, j, k), visited with i fastest
+ *                      (src/evolve.cpp:106-119), with the reference's float/double arithmetic. Used to replay
+ *                      the reference decision by decision.
+ *  MCL_SCHED_CHECKER2  two colours by parity of i+j+k (production): a different but equally valid Metropolis
+ *                      chain. The fused tiled kernel is used where the geometry allows it.
+ *  MCL_SCHED_CHECKER2_SIMPLE  two colours, one thread per site and colour, no tiling (baseline / fallback). */
+enum mcl_schedule { MCL_SCHED_REF8 = 0, MCL_SCHED_CHECKER2 = 1, MCL_SCHED_CHECKER2_SIMPLE = 2 };
+
+/* Model shared by every replica of an engine (the physics part of Parameters, include/parameters.h:18-98). */
+typedef struct mcl_model {
+  int potential;              /* mcl_potential */
+  float A, B1, C;             /* couplings (A: LL and pear; B1, C: pear) */
+  float ghrl_lambda, ghrl_mu, ghrl_nu, ghrl_rho, ghrl_sigma; /* GHRL coefficients (src/io.cpp:346-371) */
+  float field_dir[3];         /* field direction, unit length (src/main.cpp:97-106 normalises it) */
+  float elecA, elecP;         /* dielectric and dipolar couplings (src/potential.cpp:59-63) */
+  int flip_move;              /* n -> -n trial after each rotation (src/main.cpp:88: pear or elecP != 0) */
+  int n_surfaces;
+  int anch_type[MCL_MAX_SURFACES];     /* mcl_anchoring of surface s (pt = s + 2) */
+  float anch_W[MCL_MAX_SURFACES];      /* anchoring strength */
+  float anch_theta[MCL_MAX_SURFACES];  /* easy axis polar angle, degrees (rp, rp_tangent, rp_ghrl) */
+  float anch_phi[MCL_MAX_SURFACES];    /* easy axis azimuth, degrees */
+} mcl_model;
+
+/* One lattice (replica). Replicas of one engine may differ in size, temperature, field magnitude and seed. */
+typedef struct mcl_replica {
+  int nx, ny, nz;
+  int geometry;               /* mcl_geometry; slab forces z free, sphere forces all axes free */
+  int periodic[3];            /* per axis: 1 periodic, 0 free (src/potential.cpp:64-74); periodic needs even N */
+  float T;                    /* temperature (params->T) */
+  float elecE;                /* field magnitude (1 outside the electric mode) */
+  float ang_var;              /* initial rotation amplitude; the reference starts every run at 0.5 */
+  unsigned long long seed;    /* Philox key of this replica */
+} mcl_replica;
+
+/* Observables of one replica after one sweep (FP64 reductions over FP32 site terms). */
+typedef struct mcl_observables {
+  double energy;        /* mean site energy: bonds counted twice, anchoring and field once (src/evolve.cpp:33-75) */
+  double q[6];          /* mean (3 n n - I)/2: xx, xy, xz, yy, yz, zz (src/parameter_order.cpp:40-71) */
+  double S;             /* largest eigenvalue of q (src/parameter_order.cpp:19-37) */
+  double director[3];   /* its eigenvector */
+  double nsum[3];       /* sum of n over the non-empty sites */
+  double n_valid;       /* number of non-empty sites */
+  double acceptance;    /* accepted rotations / n_valid in that sweep (flips excluded, src/evolve.cpp:195) */
+  double ang_var;       /* rotation amplitude after the sweep's adaptation (src/evolve.cpp:211-220) */
+  double sweep;         /* global sweep index of the record */
+} mcl_observables;
+
+typedef struct mcl_engine mcl_engine;
+
+/* Creates an engine on the current CUDA device holding n_replicas lattices. Directors start at (0, 0, 1). */
+int mcl_create(const mcl_model *model, const mcl_replica *replicas, int n_replicas, int schedule,
+               mcl_engine **out);
+int mcl_destroy(mcl_engine *e);
+
+/* Point types (0 empty, 1 bulk, s+2 surface s) and outward normals (3 floats per site) of a sphere or custom
+ * replica, in the reference layout (src/geometry_sphere.cpp:32-58, src/geometry_custom.cpp:70-163). */
+int mcl_set_geometry(mcl_engine *e, int replica, const int *pt, const float *normals);
+
+/* Host <-> device directors of one replica (3 floats per site, reference layout). Upload rejects NaN/Inf and
+ * zero-length directors on non-empty sites with MCL_ERR_NONFINITE and leaves the device state unchanged. */
+int mcl_upload_directors(mcl_engine *e, int replica, const float *ni);
+int mcl_download_directors(mcl_engine *e, int replica, float *ni);
+
+/* Per-replica parameters; replica = -1 applies to all. */
+int mcl_set_temperature(mcl_engine *e, int replica, float T);
+int mcl_set_field(mcl_engine *e, int replica, float elecE);
+int mcl_set_ang_var(mcl_engine *e, int replica, float ang_var);
+int mcl_get_ang_var(mcl_engine *e, int replica, float *ang_var);
+/* Global sweep counter (the Philox counter of the next sweep). */
+int mcl_set_sweep_counter(mcl_engine *e, unsigned long long sweep);
+int mcl_get_sweep_counter(mcl_engine *e, unsigned long long *sweep);
+
+/* Runs n sweeps on every replica (Monte_Carlo_Step_GPU, src/evolve.cu:317-440, with ang_var adapted on the
+ * device: no host synchronisation per sweep). With measure != 0 the observables after every sweep are appended
+ * to the engine's series (energy_calculator_GPU + Q_tensor + eigen, done on the device). Asynchronous: returns
+ * after enqueueing; errors of the device work surface at the next synchronising call. */
+int mcl_sweeps(mcl_engine *e, int n, int measure);
+/* Number of records in the series; reading copies them to the host (synchronises). */
+int mcl_series_length(mcl_engine *e, int *n);
+int mcl_read_series(mcl_engine *e, int replica, int first, int count, mcl_observables *out);
+int mcl_clear_series(mcl_engine *e);
+/* Observables of the current state (synchronises). acceptance/ang_var fields refer to the last sweep. */
+int mcl_measure(mcl_engine *e, int replica, mcl_observables *out);
+int mcl_synchronize(mcl_engine *e);
+
+/* Records one byte per site for the sweeps that follow (bit 0: rotation accepted, bit 1: flip accepted,
+ * bit 7: site visited); mcl_read_decisions copies those of the last sweep. Test hook for the replay harness. */
+int mcl_record_decisions(mcl_engine *e, int enable);
+int mcl_read_decisions(mcl_engine *e, int replica, unsigned char *out);
+
+/* Work of this engine goes to `stream` (a cudaStream_t of the current device; NULL restores the engine's own
+ * stream), so a caller can order it with its own work and time it with its own events. */
+int mcl_set_stream(mcl_engine *e, void *stream);
+/* Kernel timing: with enable != 0 every following sweep records CUDA events around its sweep kernel(s) (not the
+ * per-sweep finalisation); mcl_profile_read returns their total time in ms and the number of sweeps timed, and
+ * the number of kernels this engine has launched since creation. */
+int mcl_profile(mcl_engine *e, int enable);
+int mcl_profile_read(mcl_engine *e, double *sweep_kernel_ms, long long *timed_sweeps, long long *kernel_launches);
+
+/* Runs a whole McLics input file in the current directory, like the reference program with a *GPU evolution
+ * mode (src/main.cpp:83-125): same input grammar and validation, writes ic.csv, po.dat and
+ * director_field_*.csv. The mode may be given with or without the GPU suffix. */
+int mcl_run_input_file(const char *path);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *mcl_last_error(void);
+/* Library version string. */
+const char *mcl_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

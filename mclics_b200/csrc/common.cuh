@@ -1,0 +1,121 @@
+// Shared device-side definitions: lattice layout, replica descriptors, model constants and the counter-based RNG.
+//
+// Director storage in HBM (per replica, per buffer): three FP32 component planes-of-planes (SoA),
+//   dir[off + (c * nz + z) * py * px + (y + GY) * px + (x + GX)],   c = 0, 1, 2 (x, y, z component),
+// with px = round_up(nx, 4) + 2 GX and py = ny + 2 GY. The rows carry GX = 4 cells of padding on each side and
+// the planes GY = 2 rows, so that a TMA box starting 4 cells left of a 4-aligned tile stays 16-byte aligned.
+// For a periodic axis the two cells next to each edge (x = -2, -1, nx, nx+1; likewise y) hold copies of the
+// wrapped sites ("ghosts"); the fused kernel reads them instead of wrapping. Padding beyond is zero.
+#pragma once
+#include <stdint.h>
+
+namespace mcl {
+
+constexpr int GX = 4;
+constexpr int GY = 2;
+constexpr int kMaxSurfaces = 16;
+
+enum Pot { POT_LL = 0, POT_GHRL = 1, POT_PEAR = 2 };
+enum Geo { GEO_BULK = 0, GEO_SLAB = 1, GEO_PT = 2 };  // GEO_PT: sphere and custom (point types from memory)
+enum Anch {
+  ANCH_HOMEOTROPIC = 0,
+  ANCH_RP = 1,
+  ANCH_RP_TANGENT = 2,
+  ANCH_FG = 3,
+  ANCH_HOMEOTROPIC_GHRL = 4,
+  ANCH_RP_GHRL = 5,
+  ANCH_FG_GHRL = 6
+};
+
+// Model constants, passed by value to every kernel.
+struct ModelDev {
+  int potential;
+  float A, B1, C;
+  float lam, mu, nu, rho, sigma;  // GHRL
+  float fdir[3];
+  float elecA, elecP;
+  int flip;
+  int field_on;  // elecA != 0 || elecP != 0 (the reference adds the field term only then)
+  int n_surf;
+  int anch_type[kMaxSurfaces];
+  float anch_W[kMaxSurfaces];
+  float anch_lab[kMaxSurfaces][3];  // lab easy axis, computed on the host like anchoring.cpp:19-24
+};
+
+// Immutable per-replica layout.
+struct RepDesc {
+  int nx, ny, nz;
+  int px, py;
+  int geo;           // Geo
+  int periodic[3];
+  int pad0;
+  long long off;     // float offset of this replica in the director buffers
+  long long comp;    // floats per component = nz * py * px
+  long long site_off;  // offset of this replica in the unpadded per-site arrays (pt, normals, decisions)
+  unsigned long long seed;
+  double n_valid;
+};
+
+// Mutable per-replica state (device memory).
+struct RepState {
+  float T, elecE, ang_var;
+  float pad;  // acceptance fraction of the last sweep
+  unsigned long long acc;  // accepted rotations in the current sweep
+};
+
+// One observables record (device memory, copied to mcl_observables on the host).
+struct ObsRecord {
+  double energy, q[6], S, director[3], nsum[3], n_valid, acceptance, ang_var, sweep;
+};
+// Per-block partial sums of the observables: energy, q[6], nsum[3].
+constexpr int kPartials = 10;
+
+__host__ __device__ inline long long dir_index(const RepDesc &r, int c, int x, int y, int z) {
+  return r.off + (long long)c * r.comp + ((long long)z * r.py + (y + GY)) * r.px + (x + GX);
+}
+
+// ---- Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11) ------------------------------------------------------
+// Counter (site, sweep_lo, sweep_hi, stream), key (seed_lo, seed_hi). Stream 0: plain move (u1 angle, u2 axis,
+// u3 rotation accept, u4 flip accept); stream 1: learned proposal; stream 2: initial conditions.
+struct U4 {
+  uint32_t x, y, z, w;
+};
+
+__host__ __device__ __forceinline__ U4 philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0,
+                                                      uint32_t k1) {
+#pragma unroll
+  for (int r = 0; r < 10; r++) {
+#ifdef __CUDA_ARCH__
+    uint32_t lo0 = 0xD2511F53u * c0, hi0 = __umulhi(0xD2511F53u, c0);
+    uint32_t lo1 = 0xCD9E8D57u * c2, hi1 = __umulhi(0xCD9E8D57u, c2);
+#else
+    uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+    uint32_t lo0 = (uint32_t)p0, hi0 = (uint32_t)(p0 >> 32), lo1 = (uint32_t)p1, hi1 = (uint32_t)(p1 >> 32);
+#endif
+    uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+    c0 = n0;
+    c1 = lo1;
+    c2 = n2;
+    c3 = lo0;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  return U4{c0, c1, c2, c3};
+}
+
+__host__ __device__ __forceinline__ U4 site_draws(unsigned long long seed, unsigned long long sweep, uint32_t site,
+                                                   uint32_t stream) {
+  return philox4x32_10(site, (uint32_t)sweep, (uint32_t)(sweep >> 32), stream, (uint32_t)seed, (uint32_t)(seed >> 32));
+}
+
+// 24-bit uniform in [0, 1): (x >> 8) 2^-24, exact in float and double.
+__host__ __device__ __forceinline__ float u24(uint32_t x) { return (float)(x >> 8) * (1.0f / 16777216.0f); }
+
+// Rotation axis from u2 exactly as `u2 < 0.333` / `u2 < 0.666` in double (src/evolve.cpp:156-160): for
+// u2 = m 2^-24 the tests are m < 5586813 and m < 11173626.
+__host__ __device__ __forceinline__ int rotation_axis(uint32_t x) {
+  uint32_t m = x >> 8;
+  return m < 5586813u ? 0 : (m < 11173626u ? 1 : 2);
+}
+
+}  // namespace mcl

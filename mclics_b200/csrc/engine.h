@@ -1,0 +1,82 @@
+// Engine internals shared by the C-ABI implementation (engine.cpp), the fused kernel launcher and the driver.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/mclics_b200.h"
+#include "common.cuh"
+#include "launch.h"
+
+namespace mcl {
+
+// Sets the thread's last error message and returns code.
+int fail(int code, const char *fmt, ...);
+int cuda_fail(cudaError_t err, const char *what);
+
+struct FusedPlan;  // fused tiled sweep (sweep_fused.cu)
+
+}  // namespace mcl
+
+struct mcl_engine {
+  mcl_model model_in;
+  mcl::ModelDev model;
+  int schedule = MCL_SCHED_CHECKER2;
+  int geo = mcl::GEO_BULK;
+  int n_rep = 0;
+  std::vector<mcl_replica> rep_in;
+  std::vector<mcl::RepDesc> desc;  // host copy of the layouts
+  long long dir_floats = 0;        // floats per director buffer
+  long long n_sites = 0;           // total sites over all replicas
+  long long max_sites = 0;         // largest replica
+
+  cudaStream_t stream = nullptr;
+  int device = 0;
+  mcl::RepDesc *d_desc = nullptr;
+  mcl::RepState *d_state = nullptr;
+  float *d_dir[2] = {nullptr, nullptr};
+  int cur = 0;  // which director buffer holds the current state
+  uint8_t *d_pt = nullptr;
+  float *d_nrm = nullptr;
+  float *d_stage = nullptr;  // AoS staging for upload/download (max_sites * 3 floats)
+  unsigned long long *d_sweep = nullptr;
+  unsigned int *d_done = nullptr;
+  int *d_series_len = nullptr;
+  mcl::ObsRecord *d_series = nullptr;
+  int series_cap = 0;  // rows
+  int series_len = 0;  // host mirror
+  mcl::ObsRecord *d_probe = nullptr;
+  int *d_probe_len = nullptr;  // unused length slot for probe records
+  double *d_partials = nullptr;
+  uint8_t *d_dec = nullptr;
+  bool record_dec = false;
+  bool ghosts_dirty = true;
+  bool geometry_set = true;
+
+  mcl::BlockTable half, boxes, sites;
+  std::vector<int> host_pt;  // point types (GEO_PT), for n_valid
+  mcl::FusedPlan *fused = nullptr;
+  cudaStream_t own_stream = nullptr;
+  bool profile = false;
+  std::vector<cudaEvent_t> ev_pool;  // pairs (start, stop) of timed sweeps
+  size_t ev_used = 0;
+  double prof_ms = 0;          // time of already-read event pairs
+  long long prof_sweeps = 0;
+  long long launches = 0;      // kernels launched by this engine
+
+  mcl::LaunchCtx ctx() const {
+    mcl::LaunchCtx c;
+    c.model = model;
+    c.n_replicas = n_rep;
+    c.reps = d_desc;
+    c.state = d_state;
+    c.dir = d_dir[cur];
+    c.pt = d_pt;
+    c.nrm = d_nrm;
+    c.sweep_ctr = d_sweep;
+    c.decisions = record_dec ? d_dec : nullptr;
+    c.stream = stream;
+    return c;
+  }
+};

@@ -1,0 +1,13 @@
+// Fused two-colour tiled sweep (sweep_fused.cu): both colours of a sweep in one pass over HBM.
+#pragma once
+#include "engine.h"
+
+namespace mcl {
+
+bool fused_supported(const mcl_engine *e);
+int fused_create(mcl_engine *e);
+void fused_destroy(mcl_engine *e);
+// One sweep (both colours, optional fused measurement), then the per-sweep finalisation.
+int fused_sweep(mcl_engine *e, bool measure, cudaEvent_t ev0, cudaEvent_t ev1);
+
+}  // namespace mcl

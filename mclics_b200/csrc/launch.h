@@ -1,0 +1,48 @@
+// Host-side launchers of the device kernels (implemented in the .cu files, used by engine.cpp).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace mcl {
+
+// Block work table: block b of a launch works on replica rep[b], items [base[b], base[b] + blockDim).
+struct BlockTable {
+  int n_blocks = 0;
+  int *rep = nullptr;         // device
+  long long *base = nullptr;  // device
+  int *first = nullptr;       // device, n_replicas + 1 entries: first block of each replica
+};
+
+struct LaunchCtx {
+  ModelDev model;
+  int n_replicas;
+  const RepDesc *reps;      // device
+  RepState *state;          // device
+  float *dir;               // device director buffer (current)
+  const uint8_t *pt;        // device point types (GEO_PT replicas), may be null
+  const float *nrm;         // device normals (GEO_PT replicas), may be null
+  unsigned long long *sweep_ctr;  // device
+  uint8_t *decisions;       // device, null unless recording
+  cudaStream_t stream;
+};
+
+constexpr int kThreads = 256;
+
+// One sweep with the two-colour schedule, one thread per site and colour (in place).
+cudaError_t launch_sweep_checker2_simple(const LaunchCtx &c, int geo, const BlockTable &half);
+// One sweep in the reference CPU order (8 sublattices, i fastest) with the reference arithmetic (in place).
+cudaError_t launch_sweep_ref8(const LaunchCtx &c, int geo, const BlockTable &boxes);
+// Observables of the current state into partials[block][kPartials].
+cudaError_t launch_observe(const LaunchCtx &c, int geo, const BlockTable &sites, double *partials);
+// Per-replica reduction of the partials, S by Jacobi, ang_var adaptation, series record, counter advance.
+cudaError_t launch_finalize(const LaunchCtx &c, const BlockTable &sites, const double *partials, int measure,
+                            ObsRecord *series, int *series_len, unsigned int *done_ctr);
+// Periodic ghost cells (x then y) of every replica.
+cudaError_t launch_refresh_ghosts(const LaunchCtx &c, int max_ny_nz, int max_px_nz);
+// AoS (reference layout) <-> padded SoA for one replica.
+cudaError_t launch_unpack(const LaunchCtx &c, int replica, const RepDesc &host_desc, const float *aos);
+cudaError_t launch_pack(const LaunchCtx &c, int replica, const RepDesc &host_desc, float *aos);
+
+}  // namespace mcl

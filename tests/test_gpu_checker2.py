@@ -1,0 +1,164 @@
+"""Two-colour production kernels against the oracle's two-colour sweep (same Philox draws, same state each
+sweep): decisions identical except near the acceptance threshold (FP32/FMA energies and fast exp differ from
+the oracle's reference arithmetic by ~1e-6), directors of agreeing sites within 1e-5, per-sweep FP64
+observables within the stated tolerances of the FP64 CPU oracle."""
+import zlib
+
+import numpy as np
+import pytest
+
+from helpers import M, O, explained_mismatches
+
+SEED = 0x5EED1234
+TOL = 3e-5
+
+
+def lattice_case(name):
+    """(oracle model, engine model, replica kwargs, oracle lattice, pt, ns) for a named case."""
+    rng = np.random.default_rng(zlib.crc32(name.encode()))
+    if name == "ll_bulk":
+        kw = dict(potential="ll", A=1.0)
+        geo, dims, per, T, surf = "bulk", (16, 12, 10), (1, 1, 1), 1.05, []
+    elif name == "ghrl_slab_c2":
+        kw = dict(potential="ghrl", ghrl=O.ghrl_coefficients(1, 0.5, 1.5))
+        geo, dims, per, T, surf = "slab", (16, 16, 12), (1, 1, 0), 0.8, [("homeotropic", 1.5, 0, 0)] * 2
+    elif name == "ghrl_chiral":
+        kw = dict(potential="ghrl", ghrl=O.ghrl_coefficients(1.48, 1, 2.28, 12.0))
+        geo, dims, per, T, surf = "slab", (12, 10, 8), (1, 0, 0), 0.5, [("rp_ghrl", 1.0, 90, 30), ("fg_ghrl", 1.0, 0, 0)]
+    elif name == "pear_field":
+        kw = dict(potential="pear", A=1.5, B1=0.09, C=0.3, field_dir=(0, 0, 1), elecP=0.7, elecA=0.1)
+        geo, dims, per, T, surf = "bulk", (12, 12, 12), (0, 0, 1), 0.5, []
+    elif name == "pear_slab_fg":
+        kw = dict(potential="pear", field_dir=(0, 0, 1), elecP=1.0)
+        geo, dims, per, T, surf = "slab", (16, 16, 8), (1, 1, 0), 0.5, [("fg", 1.0, 0, 0)] * 2
+    elif name == "sphere":
+        kw = dict(potential="ll")
+        geo, dims, per, T, surf = "sphere", (13, 13, 13), (0, 0, 0), 0.7, [("rp_tangent", 1.2, 30, 20)]
+    nx, ny, nz = dims
+    N = nx * ny * nz
+    pt = np.ones(N, np.int32)
+    ns = np.zeros(3 * N, np.float32)
+    if geo == "slab":
+        pt[:nx * ny] = 2
+        ns[2:3 * nx * ny:3] = -1
+        pt[-nx * ny:] = 3
+        ns[3 * (N - nx * ny) + 2::3] = 1
+    elif geo == "sphere":
+        H = np.array([nx // 2, ny // 2, nz // 2], np.float32)
+        for idx in range(N):
+            i, j, k = idx % nx, (idx // nx) % ny, idx // (nx * ny)
+            R = np.array([i, j, k], np.float32) - H
+            r = np.float32(np.sqrt(np.float32(R[0] * R[0] + R[1] * R[1] + R[2] * R[2])))
+            if r < H[2] - 1:
+                pt[idx] = 1
+            elif r < H[2] + 1:
+                pt[idx] = 2
+                ns[3 * idx:3 * idx + 3] = R / r
+            else:
+                pt[idx] = 0
+    om = O.make_model(surfaces=surf, **{k: v for k, v in kw.items()})
+    em = M.Model(surfaces=surf, **kw)
+    om.field_dir[:] = list(em.field_dir)
+    L = O.Lat(nx, ny, nz, per, pt if geo in ("slab", "sphere") else None, ns if geo in ("slab", "sphere") else None)
+    rep = dict(nx=nx, ny=ny, nz=nz, geometry=geo, periodic=per, T=T)
+    v = rng.normal(size=(N, 3)).astype(np.float32)
+    v /= np.linalg.norm(v, axis=1)[:, None]
+    ni = v.reshape(-1).astype(np.float32)
+    ni[np.repeat(pt == 0, 3)] = np.tile([0, 0, 1], int((pt == 0).sum())).astype(np.float32)
+    return om, em, rep, L, pt, ns, ni, T
+
+
+CASES = ["ll_bulk", "ghrl_slab_c2", "ghrl_chiral", "pear_field", "pear_slab_fg", "sphere"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("schedule", [M.SCHED_CHECKER2, M.SCHED_CHECKER2_SIMPLE])
+@pytest.mark.parametrize("name", CASES)
+def test_checker2_matches_oracle(name, schedule):
+    om, em, rep, L, pt, ns, ni0, T = lattice_case(name)
+    e = M.Engine(em, [M.Replica(seed=SEED, **rep)], schedule)
+    if rep["geometry"] == "sphere":
+        e.set_geometry(0, pt, ns)
+    valid = pt != 0
+    ni = ni0.copy()
+    av = 0.5
+    near_total = 0
+    for t in range(8):
+        e.upload(0, ni)
+        e.set_ang_var(av, 0)
+        e.set_sweep_counter(100 + t)
+        e.sweeps(1, measure=True)
+        got = e.download(0)
+        o = e.series(0)[-1]
+        ref = ni.copy()
+        acc, av_next, dec, margin = O.sweep(om, L, ref, T, av, SEED, 100 + t, O.SCHED_CHECKER2, True)
+        moved_gpu = np.any(got.reshape(-1, 3) != ni.reshape(-1, 3), axis=1)
+        moved_ref = np.any(ref.reshape(-1, 3) != ni.reshape(-1, 3), axis=1)
+        mism = (moved_gpu != moved_ref) & valid
+        # flips change the state too: compare the resulting orientation class as well
+        same_class = np.einsum("ij,ij->i", got.reshape(-1, 3), ref.reshape(-1, 3)) > 0.999
+        mism |= valid & ~same_class
+        hard, near = explained_mismatches(mism, margin, rep["nx"], rep["ny"], rep["nz"], L.c.periodic, TOL)
+        near_total += near
+        assert not hard, "sweep %d: unexplained mismatches %s" % (t, hard[:10])
+        agree = np.repeat(~mism, 3)
+        assert np.max(np.abs(got[agree] - ref[agree]), initial=0) <= 1e-5
+        # observables of the swept state against the FP64 oracle (computed from the device state)
+        obs = O.observables_fp64(om, L, got)
+        nv = obs[10]
+        assert o["n_valid"] == nv
+        assert abs(o["energy"] - obs[0] / nv) <= 2e-6 * max(1.0, abs(obs[0] / nv))
+        np.testing.assert_allclose(o["q"], obs[1:7] / nv, rtol=0, atol=1e-12)
+        np.testing.assert_allclose(o["nsum"], obs[7:10], rtol=0, atol=1e-9)
+        s_ref, _ = O.largest_eigen(obs[1:7] / nv)
+        assert abs(o["S"] - s_ref) < 1e-12
+        if not mism.any():
+            assert abs(o["acceptance"] * nv - acc) < 0.5
+            assert np.float32(o["ang_var"]) == np.float32(av_next)
+        ni, av = ref, av_next
+    assert near_total <= 3
+
+
+@pytest.mark.gpu
+def test_measure_matches_reference_energy():
+    """mcl_measure energy vs the reference's energy_calculator restated (float site energies, FP64 sum)."""
+    om, em, rep, L, pt, ns, ni, T = lattice_case("ghrl_slab_c2")
+    e = M.Engine(em, [M.Replica(seed=1, **rep)])
+    e.upload(0, ni)
+    o = e.measure(0)
+    assert abs(o["energy"] - O.energy_fp64sum(om, L, ni)) < 2e-6 * abs(o["energy"])
+    assert abs(o["energy"] - O.energy_ref(om, L, ni)) < 1e-5 * abs(o["energy"])
+
+
+@pytest.mark.gpu
+def test_upload_rejects_nonfinite_and_keeps_state():
+    e = M.Engine(M.Model(), [M.Replica(8, 8, 8, seed=3)])
+    ni = np.tile(np.array([0, 0, 1], np.float32), 512)
+    e.upload(0, ni)
+    bad = ni.copy()
+    bad[30] = np.nan
+    with pytest.raises(M.McLicsError) as ei:
+        e.upload(0, bad)
+    assert ei.value.code == 7
+    bad = ni.copy()
+    bad[30:33] = 0
+    with pytest.raises(M.McLicsError):
+        e.upload(0, bad)
+    assert np.array_equal(e.download(0), ni)
+
+
+@pytest.mark.gpu
+def test_same_seed_same_trajectory_other_seed_differs():
+    def run(seed):
+        e = M.Engine(M.Model(), [M.Replica(16, 16, 16, T=0.9, seed=seed)])
+        rng = np.random.default_rng(0)
+        v = rng.normal(size=(4096, 3)).astype(np.float32)
+        v /= np.linalg.norm(v, axis=1)[:, None]
+        e.upload(0, v.reshape(-1))
+        e.sweeps(20, measure=True)
+        return e.download(0), e.series(0)
+    a, sa = run(1)
+    b, sb = run(1)
+    c, _ = run(2)
+    assert np.array_equal(a, b) and np.array_equal(sa["energy"], sb["energy"])
+    assert not np.array_equal(a, c)
