@@ -148,6 +148,12 @@ int mcl_set_stream(mcl_engine *e, void *stream);
 int mcl_profile(mcl_engine *e, int enable);
 int mcl_profile_read(mcl_engine *e, double *sweep_kernel_ms, long long *timed_sweeps, long long *kernel_launches);
 
+/* Failure-detection test hook: every wait of the fused tiled sweep on a TMA copy gives up after timeout_ns
+ * (> 0 to change; default 2 s) and the sweep then reports MCL_ERR_CUDA at the next synchronising call, with
+ * the context still usable. With withhold_first_load != 0 each CTA leaves its first copy unissued, so that
+ * wait runs out; 0 restores normal operation. MCL_ERR_STATE if the engine does not use the fused sweep. */
+int mcl_debug_wait_limit(mcl_engine *e, long long timeout_ns, int withhold_first_load);
+
 /* Runs a whole McLics input file in the current directory, like the reference program with a *GPU evolution
  * mode (src/main.cpp:83-125): same input grammar and validation, writes ic.csv, po.dat and
  * director_field_*.csv. The mode may be given with or without the GPU suffix. */

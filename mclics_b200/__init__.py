@@ -94,6 +94,7 @@ def lib():
             "mcl_run_input_file": [ctypes.c_char_p],
             "mcl_set_stream": [vp, vp],
             "mcl_profile": [vp, i],
+            "mcl_debug_wait_limit": [vp, ctypes.c_longlong, i],
             "mcl_profile_read": [vp, P(ctypes.c_double), P(ctypes.c_longlong), P(ctypes.c_longlong)],
         }
         for name, args in sig.items():
@@ -278,6 +279,9 @@ class Engine:
         ms, n, k = ctypes.c_double(), ctypes.c_longlong(), ctypes.c_longlong()
         check(lib().mcl_profile_read(self._h, ctypes.byref(ms), ctypes.byref(n), ctypes.byref(k)))
         return ms.value, n.value, k.value
+
+    def debug_wait_limit(self, timeout_ns, withhold_first_load=False):
+        check(lib().mcl_debug_wait_limit(self._h, timeout_ns, 1 if withhold_first_load else 0))
 
     def record_decisions(self, on=True):
         check(lib().mcl_record_decisions(self._h, 1 if on else 0))

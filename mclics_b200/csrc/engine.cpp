@@ -434,7 +434,7 @@ int mcl_download_directors(mcl_engine *e, int replica, float *ni) {
   CK(launch_pack(e->ctx(), replica, D, e->d_stage));
   CK(cudaMemcpyAsync(ni, e->d_stage, N * 3 * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
   CK(cudaStreamSynchronize(e->stream));
-  return MCL_OK;
+  return fused_check_error(e);
 }
 
 static int set_state_field(mcl_engine *e, int replica, size_t offset, float v) {
@@ -593,6 +593,7 @@ int mcl_read_series(mcl_engine *e, int replica, int first, int count, mcl_observ
                        (size_t)e->n_rep * sizeof(ObsRecord), sizeof(ObsRecord), count, cudaMemcpyDeviceToHost,
                        e->stream));
   CK(cudaStreamSynchronize(e->stream));
+  if ((rc = fused_check_error(e))) return rc;
   for (int i = 0; i < count; i++) to_public(rows[i], out + i);
   return MCL_OK;
 }
@@ -615,6 +616,7 @@ int mcl_measure(mcl_engine *e, int replica, mcl_observables *out) {
   ObsRecord o;
   CK(cudaMemcpyAsync(&o, e->d_probe + replica, sizeof o, cudaMemcpyDeviceToHost, e->stream));
   CK(cudaStreamSynchronize(e->stream));
+  if ((rc = fused_check_error(e))) return rc;
   to_public(o, out);
   return MCL_OK;
 }
@@ -623,6 +625,13 @@ int mcl_synchronize(mcl_engine *e) {
   if (!e) return fail(MCL_ERR_ARG, "null engine");
   CK(cudaStreamSynchronize(e->stream));
   CK(cudaGetLastError());
+  return fused_check_error(e);
+}
+
+int mcl_debug_wait_limit(mcl_engine *e, long long timeout_ns, int withhold_first_load) {
+  if (!e) return fail(MCL_ERR_ARG, "null engine");
+  if (!e->fused) return fail(MCL_ERR_STATE, "this engine does not use the fused tiled sweep");
+  fused_set_test_hooks(e, timeout_ns, withhold_first_load);
   return MCL_OK;
 }
 

@@ -11,3 +11,10 @@ void fused_destroy(mcl_engine *e);
 int fused_sweep(mcl_engine *e, bool measure, cudaEvent_t ev0, cudaEvent_t ev1);
 
 }  // namespace mcl
+
+namespace mcl {
+// Reads and clears the fused kernel's error word (synchronises); MCL_ERR_CUDA if a TMA wait timed out.
+int fused_check_error(mcl_engine *e);
+// Test hook: wait limit in ns (> 0 to change) and whether the first TMA load of every CTA is withheld.
+void fused_set_test_hooks(mcl_engine *e, long long timeout_ns, int skip_first_load);
+}  // namespace mcl

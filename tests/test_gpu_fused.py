@@ -1,0 +1,128 @@
+"""The fused tiled sweep (TMA plane streaming, both colours per pass, ghost cells, ping-pong buffers) against
+the untiled two-colour kernel: same Philox draws, same physics code, so the two must agree site by site on every
+geometry the tiling has to get right (ragged last tiles, several z segments, free and periodic axes, tiny
+lattices, batches of replicas of different sizes). Also the bounded TMA wait: a withheld copy makes the wait run
+out, the error is reported at the next synchronising call and the engine keeps working."""
+import numpy as np
+import pytest
+
+from helpers import M
+
+
+def rand_dirs(n, seed):
+    rng = np.random.default_rng(seed)
+    v = rng.normal(size=(n, 3)).astype(np.float32)
+    v /= np.linalg.norm(v, axis=1)[:, None]
+    return v.reshape(-1).astype(np.float32)
+
+
+MODELS = {
+    "ll": lambda: M.Model("ll"),
+    "ghrl_slab": lambda: M.Model("ghrl", k=(1.0, 0.5, 1.5), surfaces=[("homeotropic", 1.5, 0, 0)] * 2),
+    "ghrl_chiral_rp": lambda: M.Model("ghrl", k=(1.48, 1, 2.28, 12.0),
+                                      surfaces=[("rp_ghrl", 1.0, 90, 30), ("fg_ghrl", 0.8, 0, 0)]),
+    "pear_field": lambda: M.Model("pear", A=1.5, B1=0.09, C=0.3, field_dir=(0.3, 0, 1), elecP=0.7, elecA=0.1,
+                                  surfaces=[("fg", 1.0, 0, 0), ("rp", 0.5, 40, 10)]),
+}
+
+SHAPES = [
+    # (nx, ny, nz, geometry, periodic)
+    (64, 16, 40, "bulk", (1, 1, 1)),
+    (72, 22, 70, "bulk", (1, 1, 1)),       # ragged x and y tiles, several z segments
+    (30, 18, 26, "bulk", (0, 0, 0)),       # free everywhere, odd-free sizes
+    (2, 2, 2, "bulk", (1, 1, 1)),          # smallest periodic lattice: ghosts of ghosts
+    (6, 4, 4, "bulk", (1, 0, 1)),
+    (68, 20, 33, "slab", (1, 1, 0)),
+    (16, 16, 1, "slab", (1, 1, 0)),        # single plane (surface 1 only)
+    (130, 34, 12, "slab", (0, 1, 0)),
+]
+
+
+def run(model, reps, schedule, sweeps, measure, seeds):
+    e = M.Engine(model, reps, schedule)
+    for r, rp in enumerate(reps):
+        e.upload(r, rand_dirs(rp.nx * rp.ny * rp.nz, seeds[r]))
+    e.set_sweep_counter(17)
+    e.sweeps(sweeps, measure=measure)
+    out = [e.download(r) for r in range(len(reps))]
+    ser = [e.series(r) for r in range(len(reps))] if measure else None
+    av = [e.ang_var(r) for r in range(len(reps))]
+    e.close()
+    return out, ser, av
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("model", sorted(MODELS))
+@pytest.mark.parametrize("shape", SHAPES, ids=["%dx%dx%d-%s-%s" % (s[0], s[1], s[2], s[3], "".join(map(str, s[4])))
+                                               for s in SHAPES])
+def test_fused_equals_untiled(model, shape):
+    nx, ny, nz, geo, per = shape
+    if geo == "bulk" and model in ("ghrl_slab", "ghrl_chiral_rp", "pear_field"):
+        m = MODELS[model]()
+        m.n_surfaces = 0
+    else:
+        m = MODELS[model]()
+    if geo == "slab" and m.n_surfaces < 2:
+        m = M.Model("ll", surfaces=[("homeotropic", 1.0, 0, 0), ("fg", 0.5, 0, 0)])
+    reps = [M.Replica(nx, ny, nz, geo, per, T=0.9, seed=99)]
+    a, sa, ava = run(m, reps, M.SCHED_CHECKER2, 4, True, [5])
+    b, sb, avb = run(m, reps, M.SCHED_CHECKER2_SIMPLE, 4, True, [5])
+    diff = np.abs(a[0] - b[0])
+    assert diff.max() <= 2e-6, "max director difference %g" % diff.max()
+    assert ava == avb
+    np.testing.assert_allclose(sa[0]["energy"], sb[0]["energy"], rtol=2e-6, atol=2e-6)
+    np.testing.assert_allclose(sa[0]["q"], sb[0]["q"], rtol=0, atol=1e-6)
+    np.testing.assert_array_equal(sa[0]["acceptance"], sb[0]["acceptance"])
+
+
+@pytest.mark.gpu
+def test_fused_batch_of_uneven_replicas():
+    m = M.Model("ll")
+    sizes = [(16, 16, 16), (24, 24, 24), (40, 18, 30), (8, 8, 8), (64, 32, 20)]
+    reps = [M.Replica(*s, T=1.0 + 0.05 * i, seed=100 + i) for i, s in enumerate(sizes)]
+    a, sa, ava = run(m, reps, M.SCHED_CHECKER2, 3, True, list(range(len(sizes))))
+    for i, s in enumerate(sizes):
+        b, sb, avb = run(m, [reps[i]], M.SCHED_CHECKER2_SIMPLE, 3, True, [i])
+        assert np.abs(a[i] - b[0]).max() <= 2e-6
+        np.testing.assert_allclose(sa[i]["energy"], sb[0]["energy"], rtol=2e-6)
+        assert ava[i] == avb[0]
+
+
+@pytest.mark.gpu
+def test_ghosts_and_buffers_survive_alternating_paths():
+    """Fused sweeps, then untiled ones (decision recording forces them), then fused again: the ghost cells and the
+    ping-pong buffers stay consistent with an engine that used the untiled path throughout."""
+    m = M.Model("ghrl", k=(1.0, 0.5, 1.5))
+    rp = M.Replica(40, 20, 24, "bulk", (1, 1, 1), T=0.8, seed=3)
+    e1 = M.Engine(m, [rp], M.SCHED_CHECKER2)
+    e2 = M.Engine(m, [rp], M.SCHED_CHECKER2_SIMPLE)
+    x = rand_dirs(40 * 20 * 24, 9)
+    for e in (e1, e2):
+        e.upload(0, x)
+    e1.sweeps(2)
+    e1.record_decisions(True)
+    e1.sweeps(2)
+    e1.record_decisions(False)
+    e1.sweeps(3)
+    e2.sweeps(7)
+    assert np.abs(e1.download(0) - e2.download(0)).max() <= 2e-6
+
+
+@pytest.mark.gpu
+def test_tma_wait_timeout_reports_and_recovers():
+    m = M.Model("ll")
+    rp = M.Replica(64, 32, 32, "bulk", (1, 1, 1), T=1.0, seed=1)
+    e = M.Engine(m, [rp], M.SCHED_CHECKER2)
+    x = rand_dirs(64 * 32 * 32, 1)
+    e.upload(0, x)
+    e.debug_wait_limit(100_000_000, withhold_first_load=True)  # 0.1 s
+    e.sweeps(1)
+    with pytest.raises(M.McLicsError) as ei:
+        e.synchronize()
+    assert ei.value.code == 2 and "did not complete" in str(ei.value)
+    e.debug_wait_limit(2_000_000_000, withhold_first_load=False)
+    e.upload(0, x)
+    e.sweeps(3, measure=True)
+    e.synchronize()
+    s = e.series(0)
+    assert np.all(np.isfinite(s["energy"])) and s["energy"][-1] < 0
