@@ -77,6 +77,10 @@ __device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(unsigned long long *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
   unsigned ok;
   asm volatile(
@@ -150,10 +154,14 @@ __global__ void __launch_bounds__(FT, 2) k_sweep_fused(ModelDev m, FusedArgs a) 
   auto plane_exists = [&](int p) { return perz || (p >= 0 && p < nz); };
   auto wrapz = [&](int p) { return p < 0 ? p + nz : (p >= nz ? p - nz : p); };
   auto issue = [&](int p) {  // called by thread 0 only
-    if (p > pend || !plane_exists(p)) return;
+    if (p > pend) return;
     const int lp = p - pbeg;
     if (a.skip_first_load && lp == 0) return;  // test hook: nothing will complete this barrier phase
     unsigned long long *bar = &bars[lp % NSLOT];
+    if (!plane_exists(p)) {  // no copy: complete the slot's phase anyway, so every slot advances once per use
+      mbar_arrive(bar);
+      return;
+    }
     mbar_expect_tx(bar, box_bytes);
     tma_load_plane(slots + (size_t)(lp % NSLOT) * slot_floats, map, x0, y0, wrapz(p), bar);
   };
