@@ -108,14 +108,51 @@ __host__ __device__ __forceinline__ U4 site_draws(unsigned long long seed, unsig
   return philox4x32_10(site, (uint32_t)sweep, (uint32_t)(sweep >> 32), stream, (uint32_t)seed, (uint32_t)(seed >> 32));
 }
 
-// 24-bit uniform in [0, 1): (x >> 8) 2^-24, exact in float and double.
-__host__ __device__ __forceinline__ float u24(uint32_t x) { return (float)(x >> 8) * (1.0f / 16777216.0f); }
+// ---- draws of one site -----------------------------------------------------------------------------------
+// Flip models (pear, or a dipolar field): one Philox call per site, counter (site, sweep, 0), four 24-bit fields.
+// Other models: one call per pair of same-colour sites x and x ^ 2 of a row, counter (linear index of
+// (x & ~2, y, z), sweep, 0); the site takes the 64-bit half h = (x >> 1) & 1 and splits it into three 21-bit
+// fields. Uniform = field * 2^-bits, exact in float and double.
+struct Draw {
+  uint32_t f1, f2, f3, f4;  // angle, axis, rotation acceptance, flip acceptance
+};
 
-// Rotation axis from u2 exactly as `u2 < 0.333` / `u2 < 0.666` in double (src/evolve.cpp:156-160): for
-// u2 = m 2^-24 the tests are m < 5586813 and m < 11173626.
-__host__ __device__ __forceinline__ int rotation_axis(uint32_t x) {
-  uint32_t m = x >> 8;
-  return m < 5586813u ? 0 : (m < 11173626u ? 1 : 2);
+__host__ __device__ __forceinline__ uint32_t pair_counter(uint32_t x, uint32_t y, uint32_t z, uint32_t nx, uint32_t ny) {
+  return (x & ~2u) + nx * (y + ny * z);
+}
+
+__host__ __device__ __forceinline__ Draw pair_half(const U4 &o, uint32_t h) {
+  const uint32_t lo = h ? o.z : o.x, hi = h ? o.w : o.y;
+  Draw d;
+  d.f1 = lo & 0x1FFFFFu;
+  d.f2 = ((lo >> 21) | (hi << 11)) & 0x1FFFFFu;
+  d.f3 = (hi >> 10) & 0x1FFFFFu;
+  d.f4 = 0;
+  return d;
+}
+
+__host__ __device__ __forceinline__ Draw site_draw(unsigned long long seed, unsigned long long sweep, uint32_t x,
+                                                   uint32_t y, uint32_t z, uint32_t nx, uint32_t ny, bool flip) {
+  if (flip) {
+    const U4 o = site_draws(seed, sweep, x + nx * (y + ny * z), 0);
+    return Draw{o.x >> 8, o.y >> 8, o.z >> 8, o.w >> 8};
+  }
+  return pair_half(site_draws(seed, sweep, pair_counter(x, y, z, nx, ny), 0), (x >> 1) & 1u);
+}
+
+// Field -> uniform in [0, 1): 21-bit fields for pair draws, 24-bit for flip models.
+__host__ __device__ __forceinline__ float unif(uint32_t f, bool flip) {
+  return (float)f * (flip ? (1.0f / 16777216.0f) : (1.0f / 2097152.0f));
+}
+__host__ __device__ __forceinline__ double unif_d(uint32_t f, bool flip) {
+  return (double)f * (flip ? (1.0 / 16777216.0) : (1.0 / 2097152.0));
+}
+
+// Rotation axis from the axis field exactly as `u2 < 0.333` / `u2 < 0.666` in double (src/evolve.cpp:156-160):
+// for u2 = m 2^-24 the tests are m < 5586813 and m < 11173626, for u2 = m 2^-21 m < 698352 and m < 1396704.
+__host__ __device__ __forceinline__ int rotation_axis(uint32_t m, bool flip) {
+  const uint32_t t1 = flip ? 5586813u : 698352u, t2 = flip ? 11173626u : 1396704u;
+  return m < t1 ? 0 : (m < t2 ? 1 : 2);
 }
 
 }  // namespace mcl

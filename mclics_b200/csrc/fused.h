@@ -17,4 +17,7 @@ namespace mcl {
 int fused_check_error(mcl_engine *e);
 // Test hook: wait limit in ns (> 0 to change) and whether the first TMA load of every CTA is withheld.
 void fused_set_test_hooks(mcl_engine *e, long long timeout_ns, int skip_first_load);
+// Tile configuration of the fused sweep (0: 64 x 14 tiles, 256 threads, 2 CTAs/SM; 1: 64 x 30, 512 threads).
+int fused_set_cfg(mcl_engine *e, int cfg);
+int fused_get_cfg(const mcl_engine *e, int *cfg, int *ty, int *seg, int *items);
 }  // namespace mcl

@@ -34,40 +34,22 @@ __global__ void __launch_bounds__(kThreads) k_sweep_color(ModelDev m, const RepD
     const int y = (int)(row % R.ny), z = (int)(row / R.ny);
     const int x = 2 * xh + ((colour + y + z) & 1);
     Vec3 n, nb[6], s;
-    unsigned present;
+    float w[6];
     int sid;
-    if (x < R.nx && gather_site<GEO>(R, dir, pt, nrm, x, y, z, n, nb, present, sid, s)) {
+    if (x < R.nx && gather_site_w<GEO>(R, dir, pt, nrm, x, y, z, n, nb, w, sid, s)) {
       const RepState S = st[rep];
       const float T = S.T, invT = 1.f / T;
       const long long site = site_linear(R, x, y, z);
-      const U4 r = site_draws(R.seed, *sweep_ctr, (uint32_t)site, 0);
-      const float va = (2.f * u24(r.x) - 1.f) * S.ang_var;
-      const Vec3 nn = rotate_trial(n, va, rotation_axis(r.y));
-      const float e_old = site_energy<POT>(m, n, nb, present, sid, s, S.elecE);
-      const float e_new = site_energy<POT>(m, nn, nb, present, sid, s, S.elecE);
-      Vec3 cur = n;
-      float e_cur = e_old;
-      uint8_t d = 0x80;
-      if (metropolis(u24(r.z), e_new - e_old, invT, T)) {
-        cur = nn;
-        e_cur = e_new;
-        accepted = 1;
-        d |= 1;
+      const Draw d = site_draw(R.seed, *sweep_ctr, x, y, z, R.nx, R.ny, m.flip);
+      const SiteResult r = m.flip ? site_update<POT, true>(m, n, nb, w, sid, s, S.elecE, d, S.ang_var, T, invT)
+                                  : site_update<POT, false>(m, n, nb, w, sid, s, S.elecE, d, S.ang_var, T, invT);
+      accepted = r.rot;
+      if (r.rot | r.flip) {
+        dir[dir_index(R, 0, x, y, z)] = r.n.x;
+        dir[dir_index(R, 1, x, y, z)] = r.n.y;
+        dir[dir_index(R, 2, x, y, z)] = r.n.z;
       }
-      if (m.flip) {
-        const Vec3 f{-cur.x, -cur.y, -cur.z};
-        const float e_flip = site_energy<POT>(m, f, nb, present, sid, s, S.elecE);
-        if (metropolis(u24(r.w), e_flip - e_cur, invT, T)) {
-          cur = f;
-          d |= 2;
-        }
-      }
-      if (d & 3) {
-        dir[dir_index(R, 0, x, y, z)] = cur.x;
-        dir[dir_index(R, 1, x, y, z)] = cur.y;
-        dir[dir_index(R, 2, x, y, z)] = cur.z;
-      }
-      if (dec) dec[R.site_off + site] = d;
+      if (dec) dec[R.site_off + site] = (uint8_t)(0x80u | r.rot | (r.flip << 1));
     }
   }
   const unsigned wsum = __reduce_add_sync(0xffffffffu, accepted);
@@ -100,10 +82,10 @@ __global__ void __launch_bounds__(kThreads) k_observe(ModelDev m, const RepDesc 
     const long long row = q / R.nx;
     const int y = (int)(row % R.ny), z = (int)(row / R.ny);
     Vec3 n, nb[6], s;
-    unsigned present;
+    float w[6];
     int sid;
-    if (gather_site<GEO>(R, dir, pt, nrm, x, y, z, n, nb, present, sid, s)) {
-      acc[0] = (double)site_energy<POT>(m, n, nb, present, sid, s, st[rep].elecE);
+    if (gather_site_w<GEO>(R, dir, pt, nrm, x, y, z, n, nb, w, sid, s)) {
+      acc[0] = (double)site_energy<POT>(m, n, nb, w, sid, s, st[rep].elecE);
       const double nx = n.x, ny = n.y, nz = n.z;
       acc[1] = 1.5 * nx * nx - 0.5;
       acc[2] = 1.5 * nx * ny;

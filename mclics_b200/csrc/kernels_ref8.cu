@@ -42,14 +42,15 @@ __global__ void __launch_bounds__(kThreads) k_sweep_ref8(ModelDev m, const RepDe
       const RepState S = st[rep];
       const float T = S.T;
       const long long site = site_linear(R, x, y, z);
-      const U4 r = site_draws(R.seed, *sweep_ctr, (uint32_t)site, 0);
+      const bool fl = m.flip;
+      const Draw r = site_draw(R.seed, *sweep_ctr, x, y, z, R.nx, R.ny, fl);
       // src/evolve.cpp:153-176 with the reference's double intermediate values
-      const double u1 = (double)(r.x >> 8) * (1.0 / 16777216.0);
+      const double u1 = unif_d(r.f1, fl);
       const float va = (float)((2 * u1 - 1) * (double)S.ang_var);
       const float ang = (float)(M_PI * (double)va);
       const float c = cosf(ang), sn = sinf(ang);
       float nn[3];
-      const int axis = rotation_axis(r.y);
+      const int axis = rotation_axis(r.f2, fl);
       if (axis == 0) {
         nn[0] = n[0];
         nn[1] = n[1] * c + n[2] * sn;
@@ -72,7 +73,7 @@ __global__ void __launch_bounds__(kThreads) k_sweep_ref8(ModelDev m, const RepDe
       float cur[3] = {n[0], n[1], n[2]};
       float e_cur = e_old;
       uint8_t d = 0x80;
-      const float u3 = u24(r.z);
+      const float u3 = unif(r.f3, fl);
       if (T > 0 ? u3 < expf(-(e_new - e_old) / T) : e_new <= e_old) {
         cur[0] = nn[0];
         cur[1] = nn[1];
@@ -84,7 +85,7 @@ __global__ void __launch_bounds__(kThreads) k_sweep_ref8(ModelDev m, const RepDe
       if (m.flip) {
         const float f[3] = {-cur[0], -cur[1], -cur[2]};
         const float e_flip = exact::site_energy<POT>(m, f, nb, present, sid, s, S.elecE);
-        const float u4 = u24(r.w);
+        const float u4 = unif(r.f4, fl);
         if (T > 0 ? u4 < expf(-(e_flip - e_cur) / T) : e_flip <= e_cur) {
           cur[0] = f[0];
           cur[1] = f[1];

@@ -44,6 +44,23 @@ __device__ __forceinline__ int slab_surface(int z, int nz, float &sz) {
 template <int GEO>
 __device__ __forceinline__ bool gather_site(const RepDesc &R, const float *__restrict__ dir,
                                             const uint8_t *__restrict__ pt, const float *__restrict__ nrm, int x, int y,
+                                            int z, Vec3 &n, Vec3 (&nb)[6], unsigned &present, int &sid, Vec3 &s);
+
+// The same with bond weights (1 present, 0 absent) instead of a bit mask.
+template <int GEO>
+__device__ __forceinline__ bool gather_site_w(const RepDesc &R, const float *__restrict__ dir,
+                                              const uint8_t *__restrict__ pt, const float *__restrict__ nrm, int x,
+                                              int y, int z, Vec3 &n, Vec3 (&nb)[6], float (&w)[6], int &sid, Vec3 &s) {
+  unsigned present;
+  if (!gather_site<GEO>(R, dir, pt, nrm, x, y, z, n, nb, present, sid, s)) return false;
+#pragma unroll
+  for (int d = 0; d < 6; d++) w[d] = (present >> d) & 1u ? 1.f : 0.f;
+  return true;
+}
+
+template <int GEO>
+__device__ __forceinline__ bool gather_site(const RepDesc &R, const float *__restrict__ dir,
+                                            const uint8_t *__restrict__ pt, const float *__restrict__ nrm, int x, int y,
                                             int z, Vec3 &n, Vec3 (&nb)[6], unsigned &present, int &sid, Vec3 &s) {
   const long long site = site_linear(R, x, y, z);
   int p = 1;

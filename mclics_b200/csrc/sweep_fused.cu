@@ -21,7 +21,10 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <stdlib.h>
+
 #include <algorithm>
+#include <cmath>
 #include <vector>
 
 #include "fused.h"
@@ -32,7 +35,6 @@ namespace mcl {
 
 constexpr int FT = 256;      // threads per CTA
 constexpr int NSLOT = 6;     // plane slots (4 live + 2 in flight)
-constexpr int kMaxTX = 64, kMaxTY = 32;
 
 struct FusedItem {
   int rep, x0, y0, z0, z1;
@@ -48,13 +50,20 @@ struct FusedArgs {
   const unsigned long long *sweep_ctr;
   unsigned int *err;            // error word (bit 0: TMA wait timeout)
   int cur;                      // buffer read by this sweep (selects the tensor map)
-  int tx, ty;                   // tile size
+  int measure;                  // fuse the observables
   long long timeout_ns;
   int skip_first_load;          // test hook: never issue the first TMA load (its wait must time out)
 };
 
+// Tile configurations: rows per tile and threads per CTA (64 columns always).
+struct FusedCfg {
+  int ty, nt, ctas_per_sm;
+};
+static const FusedCfg kCfgs[] = {{14, 256, 2}, {30, 512, 1}};
+constexpr int kNumCfgs = 2;
+
 struct FusedPlan {
-  int tx = 64, ty = 16, seg = 32;
+  int cfg = 0, tx = 64, ty = 14, seg = 32;
   int n_items = 0;
   FusedItem *d_items = nullptr;
   CUtensorMap *d_tmaps = nullptr;
@@ -117,305 +126,396 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, unsig
 }
 
 // ---- the kernel --------------------------------------------------------------------------------------------
-// Shared memory: NSLOT plane slots of 3 * (tx + 8) * (ty + 4) floats, then NSLOT mbarriers.
-template <int POT, int GEO, bool MEASURE>
-__global__ void __launch_bounds__(FT, 2) k_sweep_fused(ModelDev m, FusedArgs a) {
+// Tile: TX = 64 columns (16 groups of 4 cells) x TY rows. Window in shared memory: W = TX + 8 columns (x0 - 4 ..
+// x0 + TX + 3) by H = TY + 4 rows (y0 - 2 .. y0 + TY + 1), three component planes, one TMA box per slot.
+constexpr int TXF = 64, NG = TXF / 4, WF = TXF + 8, NSL = 7;
+
+template <int TY>
+struct Win {
+  static constexpr int W = WF, H = TY + 4, PF = W * H, SLOT = (3 * PF + 31) / 32 * 32;
+};
+
+__device__ __forceinline__ float elem(const float4 &v, int e) {  // e is a compile-time constant at every call
+  return e == 0 ? v.x : (e == 1 ? v.y : (e == 2 ? v.z : v.w));
+}
+__device__ __forceinline__ void set_elem(float4 &v, int e, float x) {
+  if (e == 0) v.x = x;
+  else if (e == 1) v.y = x;
+  else if (e == 2) v.z = x;
+  else v.w = x;
+}
+
+// Geometry/boundary facts of a work item that the site updates need.
+struct Ctx {
+  int nx, ny, nz;
+  bool perx, pery;
+  unsigned long long seed, sweep;
+  float T, invT, av, elecE;
+};
+
+// One task: the two sites (xg + E, y) and (xg + E + 2, y) of one colour in the 4-cell group starting at window
+// column wc (= xg - x0 + 4) of window row wy. v0 / v1: whether each site is to be updated. Returns the updated
+// group back into shared memory; adds the accepted rotations of counted sites and (bond, single) of measured sites.
+template <int POT, int GEO, bool FLIP, int TY, int E>
+__device__ __forceinline__ void pair_task(const ModelDev &m, const Ctx &c, float *cs, const float *below,
+                                          const float *above, int wy, int wc, int xg, int y, int zw, bool v0, bool v1,
+                                          bool count, bool meas_b, unsigned &accepted, float &e_acc) {
+  constexpr int W = Win<TY>::W, PF = Win<TY>::PF;
+  float *row = cs + wy * W + wc;
+  float4 o[3], yu[3], yd[3], zu[3], zd[3];
+  float ex[3];
+#pragma unroll
+  for (int q = 0; q < 3; q++) {
+    o[q] = *reinterpret_cast<const float4 *>(row + q * PF);
+    yu[q] = *reinterpret_cast<const float4 *>(row + q * PF + W);
+    yd[q] = *reinterpret_cast<const float4 *>(row + q * PF - W);
+    ex[q] = E == 0 ? row[q * PF - 1] : row[q * PF + 4];
+  }
+  const float wz_up = above ? 1.f : 0.f, wz_dn = below ? 1.f : 0.f;
+  const float *rowu = above ? above + wy * W + wc : row, *rowd = below ? below + wy * W + wc : row;
+#pragma unroll
+  for (int q = 0; q < 3; q++) {
+    zu[q] = *reinterpret_cast<const float4 *>(rowu + q * PF);
+    zd[q] = *reinterpret_cast<const float4 *>(rowd + q * PF);
+  }
+  // surface of this plane (slab): uniform per plane
+  int sid = -1;
+  Vec3 sn{0.f, 0.f, 0.f};
+  if (GEO == GEO_SLAB) {
+    float sz;
+    sid = slab_surface(zw, c.nz, sz);
+    sn.z = sz;
+  }
+  const int yw = c.pery ? (y < 0 ? y + c.ny : (y >= c.ny ? y - c.ny : y)) : y;
+  const float wyp = (c.pery || y + 1 < c.ny) ? 1.f : 0.f, wym = (c.pery || y - 1 >= 0) ? 1.f : 0.f;
+  SiteResult r[2];
+  Draw d[2];
+  int xs[2] = {xg + E, xg + E + 2};
+  int xw[2];
+#pragma unroll
+  for (int s = 0; s < 2; s++) xw[s] = c.perx ? (xs[s] < 0 ? xs[s] + c.nx : (xs[s] >= c.nx ? xs[s] - c.nx : xs[s])) : xs[s];
+  if (FLIP) {
+#pragma unroll
+    for (int s = 0; s < 2; s++) d[s] = site_draw(c.seed, c.sweep, xw[s], yw, zw, c.nx, c.ny, true);
+  } else {
+    // one Philox call for the pair: both sites share x & ~2 unless a periodic wrap split them (ring columns)
+    const int sv = v0 ? 0 : 1;
+    const U4 out = site_draws(c.seed, c.sweep, pair_counter(xw[sv], yw, zw, c.nx, c.ny), 0);
+    d[0] = pair_half(out, (xw[0] >> 1) & 1u);
+    d[1] = pair_half(out, (xw[1] >> 1) & 1u);
+  }
+#pragma unroll
+  for (int s = 0; s < 2; s++) {
+    const int e = E + 2 * s;  // element of the site in the group
+    const Vec3 n{elem(o[0], e), elem(o[1], e), elem(o[2], e)};
+    Vec3 nb[6];
+    // +x: element e+1 (or the extra cell for E = 1, s = 1); -x: element e-1 (or the extra cell for E = 0, s = 0)
+    if (e + 1 <= 3)
+      nb[0] = Vec3{elem(o[0], e + 1), elem(o[1], e + 1), elem(o[2], e + 1)};
+    else
+      nb[0] = Vec3{ex[0], ex[1], ex[2]};
+    if (e - 1 >= 0)
+      nb[1] = Vec3{elem(o[0], e - 1), elem(o[1], e - 1), elem(o[2], e - 1)};
+    else
+      nb[1] = Vec3{ex[0], ex[1], ex[2]};
+    nb[2] = Vec3{elem(yu[0], e), elem(yu[1], e), elem(yu[2], e)};
+    nb[3] = Vec3{elem(yd[0], e), elem(yd[1], e), elem(yd[2], e)};
+    nb[4] = Vec3{elem(zu[0], e), elem(zu[1], e), elem(zu[2], e)};
+    nb[5] = Vec3{elem(zd[0], e), elem(zd[1], e), elem(zd[2], e)};
+    const float w[6] = {(c.perx || xs[s] + 1 < c.nx) ? 1.f : 0.f, (c.perx || xs[s] - 1 >= 0) ? 1.f : 0.f, wyp, wym,
+                        wz_up, wz_dn};
+    r[s] = site_update<POT, FLIP>(m, n, nb, w, sid, sn, c.elecE, d[s], c.av, c.T, c.invT);
+  }
+  if (v0 | v1) {
+    if (v0) {
+      set_elem(o[0], E, r[0].n.x);
+      set_elem(o[1], E, r[0].n.y);
+      set_elem(o[2], E, r[0].n.z);
+    }
+    if (v1) {
+      set_elem(o[0], E + 2, r[1].n.x);
+      set_elem(o[1], E + 2, r[1].n.y);
+      set_elem(o[2], E + 2, r[1].n.z);
+    }
+#pragma unroll
+    for (int q = 0; q < 3; q++) *reinterpret_cast<float4 *>(row + q * PF) = o[q];
+  }
+  if (count) accepted += (v0 ? r[0].rot : 0u) + (v1 ? r[1].rot : 0u);
+  if (meas_b) {
+    if (v0) e_acc += fmaf(2.f, r[0].bond, r[0].single);
+    if (v1) e_acc += fmaf(2.f, r[1].bond, r[1].single);
+  }
+}
+
+template <int POT, int GEO, bool FLIP, int TY, int NT>
+__global__ void __launch_bounds__(NT, NT <= 256 ? 2 : 1) k_sweep_fused(ModelDev m, FusedArgs a) {
+  constexpr int W = Win<TY>::W, PF = Win<TY>::PF, SLOT = Win<TY>::SLOT;
   extern __shared__ __align__(128) unsigned char smem_dyn[];
   unsigned char *smem_raw = (unsigned char *)(((uintptr_t)smem_dyn + 127) & ~(uintptr_t)127);
+  float *slots = reinterpret_cast<float *>(smem_raw);
+  unsigned long long *bars = reinterpret_cast<unsigned long long *>(smem_raw + (size_t)NSL * SLOT * 4);
+  __shared__ int s_fail;
   const FusedItem it = a.items[blockIdx.x];
   const RepDesc R = a.reps[it.rep];
   const RepState S = a.st[it.rep];
-  const int TX = a.tx, TY = a.ty;
-  const int W = TX + 8, H = TY + 4;      // slot row length and rows
-  const int plane_floats = W * H;        // one component
-  const int slot_floats = ((3 * plane_floats + 31) / 32) * 32;  // slots start on 128-byte boundaries
-  float *slots = reinterpret_cast<float *>(smem_raw);
-  unsigned long long *bars = reinterpret_cast<unsigned long long *>(smem_raw + (size_t)NSLOT * slot_floats * 4);
-  __shared__ int s_fail;
   const int tid = threadIdx.x;
   const CUtensorMap *map = a.tmaps + 2 * it.rep + a.cur;
-  const unsigned long long sweep = *a.sweep_ctr;
   const int nx = R.nx, ny = R.ny, nz = R.nz;
-  const bool perx = R.periodic[0], pery = R.periodic[1], perz = R.periodic[2];
+  const bool perz = R.periodic[2];
   const int x0 = it.x0, y0 = it.y0, z0 = it.z0, z1 = it.z1;
-  const float T = S.T, invT = 1.f / T, av = S.ang_var, elecE = S.elecE;
-  const unsigned box_bytes = (unsigned)(3 * plane_floats) * 4u;
+  const bool measure = a.measure != 0;
+  Ctx c;
+  c.nx = nx;
+  c.ny = ny;
+  c.nz = nz;
+  c.perx = R.periodic[0];
+  c.pery = R.periodic[1];
+  c.seed = R.seed;
+  c.sweep = *a.sweep_ctr;
+  c.T = S.T;
+  c.invT = 1.f / S.T;
+  c.av = S.ang_var;
+  c.elecE = S.elecE;
+  constexpr unsigned box_bytes = 3u * PF * 4u;
 
   if (tid == 0) {
     s_fail = 0;
-    for (int q = 0; q < NSLOT; q++) mbar_init(&bars[q], 1);
+    for (int q = 0; q < NSL; q++) mbar_init(&bars[q], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("prefetch.tensormap [%0];" ::"l"(map) : "memory");
   }
   __syncthreads();
 
-  // plane p (local index lp = p - (z0 - 2)) lives in slot lp % NSLOT; exists unless free z and p outside [0, nz)
-  const int pbeg = z0 - 2, pend = z1 + 1;  // inclusive range of planes used
+  // Plane p (local index lp = p - pbeg) lives in slot lp % NSL; every use of a slot completes one barrier phase.
+  const int pbeg = z0 - 2, pend = z1 + 1;
   auto plane_exists = [&](int p) { return perz || (p >= 0 && p < nz); };
   auto wrapz = [&](int p) { return p < 0 ? p + nz : (p >= nz ? p - nz : p); };
-  auto issue = [&](int p) {  // called by thread 0 only
+  auto slot_ptr = [&](int p) -> float * { return slots + (size_t)((p - pbeg) % NSL) * SLOT; };
+  int last_issued = pbeg - 1;  // meaningful in thread 0 only
+  auto issue = [&](int p) {    // thread 0 only
     if (p > pend) return;
     const int lp = p - pbeg;
+    last_issued = p;
     if (a.skip_first_load && lp == 0) return;  // test hook: nothing will complete this barrier phase
-    unsigned long long *bar = &bars[lp % NSLOT];
-    if (!plane_exists(p)) {  // no copy: complete the slot's phase anyway, so every slot advances once per use
+    unsigned long long *bar = &bars[lp % NSL];
+    if (!plane_exists(p)) {  // no copy: complete the slot's phase anyway
       mbar_arrive(bar);
       return;
     }
     mbar_expect_tx(bar, box_bytes);
-    tma_load_plane(slots + (size_t)(lp % NSLOT) * slot_floats, map, x0, y0, wrapz(p), bar);
+    tma_load_plane(slot_ptr(p), map, x0, y0, wrapz(p), bar);
   };
-  // Slot reuse: at step k the CTA reads planes k-2 .. k+1; plane k+3 goes into the slot of plane k-3, whose last
-  // reader was step k-1. Four planes are issued before the loop, one per step after that.
-  int last_issued = pbeg - 1;
-  if (tid == 0) {
-    for (int p = pbeg; p <= pbeg + 3 && p <= pend; p++) issue(p);
-    last_issued = min(pend, pbeg + 3);
-  }
-
-  auto wait_plane = [&](int p) -> bool {  // every thread waits; returns false if the CTA must bail out
-    if (p <= pend && plane_exists(p)) {
+  int waited = pbeg - 1;  // uniform: highest plane waited for successfully
+  auto wait_plane = [&](int p) -> bool {
+    if (p <= pend && p > waited) {
       const int lp = p - pbeg;
-      const unsigned parity = (unsigned)((lp / NSLOT) & 1);
-      if (!mbar_wait_bounded(&bars[lp % NSLOT], parity, a.timeout_ns)) s_fail = 1;
+      if (plane_exists(p) && !mbar_wait_bounded(&bars[lp % NSL], (unsigned)((lp / NSL) & 1), a.timeout_ns)) s_fail = 1;
     }
     __syncthreads();
-    return s_fail == 0;
+    if (s_fail) return false;
+    if (p > waited) waited = p;
+    return true;
   };
-
-  // slot base pointers
-  auto slot_of = [&](int p) -> const float * { return slots + (size_t)((p - pbeg) % NSLOT) * slot_floats; };
-  auto slot_of_w = [&](int p) -> float * { return slots + (size_t)((p - pbeg) % NSLOT) * slot_floats; };
-  // cell (x, y) of the tile's padded window: column x - (x0 - 4), row y - (y0 - 2)
-  auto cell = [&](int x, int y) { return (y - y0 + 2) * W + (x - x0 + 4); };
+  // Slot reuse: at step k the CTA reads planes k-3 .. k+1; plane k+3 goes into the slot of plane k-4, whose last
+  // reader was step k-1 (the barrier at the start of step k separates them).
+  if (tid == 0)
+    for (int p = pbeg; p <= pbeg + 3; p++) issue(p);
 
   unsigned accepted = 0;
-  double acc_e = 0, acc_q[6] = {0, 0, 0, 0, 0, 0}, acc_n[3] = {0, 0, 0};
-
-  // one trial move of site (x, y, z) (unwrapped coordinates inside the window), director in slot `cur`
-  auto update = [&](int x, int y, int z, float *cs, const float *below, const float *above, bool count,
-                    float *bond_out, float *single_out) {
-    const int c = cell(x, y);
-    Vec3 n{cs[c], cs[c + plane_floats], cs[c + 2 * plane_floats]};
-    Vec3 nb[6];
-    unsigned present = 0;
-    const int xw = perx ? (x < 0 ? x + nx : (x >= nx ? x - nx : x)) : x;
-    const int yw = pery ? (y < 0 ? y + ny : (y >= ny ? y - ny : y)) : y;
-    const int zw = perz ? (z < 0 ? z + nz : (z >= nz ? z - nz : z)) : z;
-    // +x, -x, +y, -y in plane; +z (above), -z (below)
-    const int offs[4] = {1, -1, W, -W};
+  double dacc[kPartials];
 #pragma unroll
-    for (int d = 0; d < 4; d++) {
-      bool ok;
-      if (d == 0) ok = perx || xw + 1 < nx;
-      else if (d == 1) ok = perx || xw - 1 >= 0;
-      else if (d == 2) ok = pery || yw + 1 < ny;
-      else ok = pery || yw - 1 >= 0;
-      const int q = c + offs[d];
-      nb[d] = Vec3{cs[q], cs[q + plane_floats], cs[q + 2 * plane_floats]};
-      present |= ok ? (1u << d) : 0u;
-    }
-    if (above) {
-      nb[4] = Vec3{above[c], above[c + plane_floats], above[c + 2 * plane_floats]};
-      present |= 16u;
-    } else {
-      nb[4] = Vec3{0.f, 0.f, 0.f};
-    }
-    if (below) {
-      nb[5] = Vec3{below[c], below[c + plane_floats], below[c + 2 * plane_floats]};
-      present |= 32u;
-    } else {
-      nb[5] = Vec3{0.f, 0.f, 0.f};
-    }
-    int sid = -1;
-    Vec3 s{0.f, 0.f, 0.f};
-    if (GEO == GEO_SLAB) {
-      float sz;
-      sid = slab_surface(zw, nz, sz);
-      s.z = sz;
-    }
-    const uint32_t site = (uint32_t)xw + (uint32_t)nx * ((uint32_t)yw + (uint32_t)ny * (uint32_t)zw);
-    const U4 r = site_draws(R.seed, sweep, site, 0);
-    const float va = (2.f * u24(r.x) - 1.f) * av;
-    const Vec3 nn = rotate_trial(n, va, rotation_axis(r.y));
-    const float b_old = bond_sum<POT>(m, n, nb, present), b_new = bond_sum<POT>(m, nn, nb, present);
-    float s_old = 0.f, s_new = 0.f;
-    if (sid >= 0) {
-      s_old = anchoring_energy(m, sid, n, s);
-      s_new = anchoring_energy(m, sid, nn, s);
-    }
-    if (m.field_on) {
-      s_old += field_energy(m, n, elecE);
-      s_new += field_energy(m, nn, elecE);
-    }
-    const float e_old = b_old + s_old, e_new = b_new + s_new;
-    Vec3 curv = n;
-    float e_cur = e_old, b_cur = b_old, s_cur = s_old;
-    bool moved = false;
-    if (metropolis(u24(r.z), e_new - e_old, invT, T)) {
-      curv = nn;
-      e_cur = e_new;
-      b_cur = b_new;
-      s_cur = s_new;
-      moved = true;
-      if (count) accepted++;
-    }
-    if (m.flip) {
-      const Vec3 f{-curv.x, -curv.y, -curv.z};
-      const float bf = bond_sum<POT>(m, f, nb, present);
-      float sf = 0.f;
-      if (sid >= 0) sf = anchoring_energy(m, sid, f, s);
-      if (m.field_on) sf += field_energy(m, f, elecE);
-      if (metropolis(u24(r.w), (bf + sf) - e_cur, invT, T)) {
-        curv = f;
-        b_cur = bf;
-        s_cur = sf;
-        moved = true;
-      }
-    }
-    if (moved) {
-      cs[c] = curv.x;
-      cs[c + plane_floats] = curv.y;
-      cs[c + 2 * plane_floats] = curv.z;
-    }
-    if (bond_out) *bond_out = b_cur;
-    if (single_out) *single_out = s_cur;
-  };
+  for (int q = 0; q < kPartials; q++) dacc[q] = 0.0;
+
+  // ring column limits (colour A of owned planes): left x0 - 1, right min(x0 + TX, nx) (periodic) / x0 + TX
+  const bool has_left = c.perx || x0 >= 1;
+  const int xright = c.perx ? min(x0 + TXF, nx) : x0 + TXF;
+  const bool has_right = xright < nx || (c.perx && xright == nx);
+  const int ylim_ring = c.pery ? ny : ny - 1;  // highest valid ring row
 
   bool ok = wait_plane(z0 - 2) && wait_plane(z0 - 1);
-  // ring limits: sites that exist (free axes) or whose ghost data is valid (periodic axes)
-  const int xr_lo = max(x0 - 1, perx ? -1 : 0), xr_hi = min(x0 + TX, perx ? nx : nx - 1);
-  const int yr_lo = max(y0 - 1, pery ? -1 : 0), yr_hi = min(y0 + TY, pery ? ny : ny - 1);
-  int k = z0 - 1;
-  for (; ok && k <= z1; k++) {
-    ok = wait_plane(k + 1);  // planes k-2 .. k+1 are resident after this
+  for (int k = z0 - 1; ok && k <= z1 + 2; k++) {
+    ok = wait_plane(k + 1);
     if (!ok) break;
-    if (tid == 0 && k + 3 <= pend) {
-      issue(k + 3);
-      last_issued = k + 3;
-    }
-    // (a) colour A of plane k on the tile plus a one-site ring
-    if (plane_exists(k)) {
-      float *cs = slot_of_w(k);
-      const float *below = plane_exists(k - 1) ? slot_of(k - 1) : nullptr;
-      const float *above = plane_exists(k + 1) ? slot_of(k + 1) : nullptr;
-      const int rw = TX + 2, nrow = TY + 2, half = (rw + 1) / 2;
-      for (int q = tid; q < half * nrow; q += FT) {
-        const int row = q / half, j = q % half;
-        const int y = y0 - 1 + row;
-        const int xs = x0 - 1;
-        const int x = xs + 2 * j + ((xs + y + k) & 1);  // parity 0 sites of the row
-        if (x < xr_lo || x > xr_hi || y < yr_lo || y > yr_hi) continue;
-        const bool interior = x >= x0 && x < x0 + TX && y >= y0 && y < y0 + TY && x < nx && y < ny && k >= z0 &&
-                              k < z1;
-        update(x, y, k, cs, below, above, interior, nullptr, nullptr);
+    if (tid == 0) issue(k + 3);
+    // ---- phase: colour A of plane k, colour B of plane k - 2 (independent), then write-out of plane k - 3
+    const bool doA = k <= z1 && plane_exists(k);
+    const bool ownA = k >= z0 && k < z1;
+    const int kb = k - 2;
+    const bool doB = kb >= z0 && kb < z1 && plane_exists(kb);
+    const int rowsA = doA ? (ownA ? TY + 2 : TY) : 0;
+    const int row0A = ownA ? y0 - 1 : y0;
+    const int nAg = rowsA * NG;
+    const int nAc = (doA && ownA) ? TY : 0;  // TY/2 ring sites on each side
+    const int nB = doB ? TY * NG : 0;
+    const int ntask = nAg + nAc + nB;
+    const int zwA = wrapz(k), zwB = wrapz(kb);
+    float *csA = doA ? slot_ptr(k) : nullptr;
+    const float *belowA = (doA && plane_exists(k - 1)) ? slot_ptr(k - 1) : nullptr;
+    const float *aboveA = (doA && plane_exists(k + 1)) ? slot_ptr(k + 1) : nullptr;
+    float *csB = doB ? slot_ptr(kb) : nullptr;
+    const float *belowB = (doB && plane_exists(kb - 1)) ? slot_ptr(kb - 1) : nullptr;
+    const float *aboveB = (doB && plane_exists(kb + 1)) ? slot_ptr(kb + 1) : nullptr;
+    float eB = 0.f;
+    for (int t = tid; t < ntask; t += NT) {
+      if (t < nAg) {
+        // rows in parity order (even-offset rows first) so that warps see one element offset E
+        const int half_rows = (rowsA + 1) / 2;
+        const int rr = t / NG, g = t % NG;
+        const int ri = rr < half_rows ? 2 * rr : 2 * (rr - half_rows) + 1;
+        const int y = row0A + ri;
+        const int xg = x0 + 4 * g;
+        const bool yok = ownA ? (y >= (c.pery ? -1 : 0) && y <= ylim_ring && !(y >= ny && y != ny)) : (y < ny);
+        const bool yint = y >= y0 && y < y0 + TY && y < ny;
+        const int E = (y + k) & 1;  // colour A: x + y + k even, xg is a multiple of 4
+        const bool v0 = yok && xg + E < nx, v1 = yok && xg + E + 2 < nx;
+        const int wy = y - y0 + 2, wc = xg - x0 + 4;
+        if (E == 0)
+          pair_task<POT, GEO, FLIP, TY, 0>(m, c, csA, belowA, aboveA, wy, wc, xg, y, zwA, v0, v1, ownA && yint, false,
+                                           accepted, eB);
+        else
+          pair_task<POT, GEO, FLIP, TY, 1>(m, c, csA, belowA, aboveA, wy, wc, xg, y, zwA, v0, v1, ownA && yint, false,
+                                           accepted, eB);
+      } else if (t < nAg + nAc) {
+        // ring columns: one site each, left side first
+        const int q = t - nAg, side = q / (TY / 2), j = q % (TY / 2);
+        const int xc = side == 0 ? x0 - 1 : xright;
+        const int y = y0 + 2 * j + ((xc + y0 + k) & 1);  // (xc + y + k) even
+        const bool valid = (side == 0 ? has_left : has_right) && y < y0 + TY && y < ny;
+        const int xg = xc & ~3;  // floor to the group (xc may be -1)
+        const int e = xc - xg;
+        const int E = e & 1;
+        const int wy = y - y0 + 2, wc = xg - x0 + 4;
+        const bool v0 = valid && e == E, v1 = valid && e == E + 2;
+        if (E == 0)
+          pair_task<POT, GEO, FLIP, TY, 0>(m, c, csA, belowA, aboveA, wy, wc, xg, y, zwA, v0, v1, false, false,
+                                           accepted, eB);
+        else
+          pair_task<POT, GEO, FLIP, TY, 1>(m, c, csA, belowA, aboveA, wy, wc, xg, y, zwA, v0, v1, false, false,
+                                           accepted, eB);
+      } else {
+        const int tb = t - nAg - nAc;
+        const int half_rows = (TY + 1) / 2;
+        const int rr = tb / NG, g = tb % NG;
+        const int ri = rr < half_rows ? 2 * rr : 2 * (rr - half_rows) + 1;
+        const int y = y0 + ri;
+        const int xg = x0 + 4 * g;
+        const int E = (y + kb + 1) & 1;  // colour B: x + y + kb odd
+        const bool yok = y < ny;
+        const bool v0 = yok && xg + E < nx, v1 = yok && xg + E + 2 < nx;
+        const int wy = y - y0 + 2, wc = xg - x0 + 4;
+        if (E == 0)
+          pair_task<POT, GEO, FLIP, TY, 0>(m, c, csB, belowB, aboveB, wy, wc, xg, y, zwB, v0, v1, true, measure,
+                                           accepted, eB);
+        else
+          pair_task<POT, GEO, FLIP, TY, 1>(m, c, csB, belowB, aboveB, wy, wc, xg, y, zwB, v0, v1, true, measure,
+                                           accepted, eB);
       }
     }
-    __syncthreads();
-    // (b) colour B of plane k - 1 (owned planes only), (c) write-out of plane k - 1
-    const int pb = k - 1;
-    if (pb >= z0 && pb < z1 && plane_exists(pb)) {
-      float *cs = slot_of_w(pb);
-      const float *below = plane_exists(pb - 1) ? slot_of(pb - 1) : nullptr;
-      const float *above = plane_exists(pb + 1) ? slot_of(pb + 1) : nullptr;
-      const int half = TX / 2;
-      for (int q = tid; q < half * TY; q += FT) {
-        const int row = q / half, j = q % half;
-        const int y = y0 + row;
-        const int x = x0 + 2 * j + ((x0 + y + pb + 1) & 1);  // parity 1 sites
-        if (x >= nx || y >= ny) continue;
-        float bnd, sgl;
-        update(x, y, pb, cs, below, above, true, &bnd, &sgl);
-        if (MEASURE) acc_e += (double)(2.f * bnd + sgl);
-      }
-      __syncthreads();
-      // (c) write-out (both colours) and site terms of colour A
-      const int zw = pb < 0 ? pb + nz : (pb >= nz ? pb - nz : pb);
-      for (int q = tid; q < TX * TY; q += FT) {
-        const int row = q / TX, col = q % TX;
-        const int y = y0 + row, x = x0 + col;
-        if (x >= nx || y >= ny) continue;
-        const int c = cell(x, y);
-        const float vx = cs[c], vy = cs[c + plane_floats], vz = cs[c + 2 * plane_floats];
-        const long long base = R.off + ((long long)zw * R.py) * R.px;
-        // the site and its ghost images along periodic axes (x + nx for x < 2, x - nx for x >= nx - 2)
-        int xs_[3] = {x, 0, 0}, ys_[3] = {y, 0, 0}, ncx = 1, ncy = 1;
-        if (perx) {
-          if (x < 2) xs_[ncx++] = x + nx;
-          if (x >= nx - 2) xs_[ncx++] = x - nx;
+    if (measure) dacc[0] += (double)eB;
+    // ---- write-out of plane k - 3 (both colours final) and its site terms
+    const int kw = k - 3;
+    if (kw >= z0 && kw < z1 && plane_exists(kw)) {
+      const float *cw = slot_ptr(kw);
+      const int zw = wrapz(kw);
+      const long long pbase = R.off + (long long)zw * R.py * R.px;
+      int sid = -1;
+      float sz = 0.f;
+      if (GEO == GEO_SLAB) sid = slab_surface(zw, nz, sz);
+      for (int t = tid; t < TY * NG; t += NT) {
+        const int rr = t / NG, g = t % NG;
+        const int y = y0 + rr, xg = x0 + 4 * g;
+        if (y >= ny || xg >= nx) continue;
+        const int wy = rr + 2, wc = 4 * g + 4;
+        float4 v[3];
+#pragma unroll
+        for (int q = 0; q < 3; q++) v[q] = *reinterpret_cast<const float4 *>(cw + q * PF + wy * W + wc);
+        const bool full = xg + 3 < nx;
+        // the row itself and its ghost rows along a periodic y
+        int yrows[3] = {y, 0, 0}, nyr = 1;
+        if (c.pery) {
+          if (y < 2) yrows[nyr++] = y + ny;
+          if (y >= ny - 2) yrows[nyr++] = y - ny;
         }
-        if (pery) {
-          if (y < 2) ys_[ncy++] = y + ny;
-          if (y >= ny - 2) ys_[ncy++] = y - ny;
-        }
-        for (int ix = 0; ix < ncx; ix++)
-          for (int iy = 0; iy < ncy; iy++) {
-            const long long o = base + (long long)(ys_[iy] + GY) * R.px + (xs_[ix] + GX);
-            a.out[o] = vx;
-            a.out[o + R.comp] = vy;
-            a.out[o + 2 * R.comp] = vz;
+        for (int iy = 0; iy < nyr; iy++) {
+          float *dst = a.out + pbase + (long long)(yrows[iy] + GY) * R.px + (xg + GX);
+          if (full) {
+#pragma unroll
+            for (int q = 0; q < 3; q++) *reinterpret_cast<float4 *>(dst + q * R.comp) = v[q];
+          } else {
+            for (int e = 0; e < 4 && xg + e < nx; e++)
+#pragma unroll
+              for (int q = 0; q < 3; q++) dst[q * R.comp + e] = elem(v[q], e);
           }
-        if (MEASURE) {
-          const double dx = vx, dy = vy, dz = vz;
-          acc_q[0] += 1.5 * dx * dx - 0.5;
-          acc_q[1] += 1.5 * dx * dy;
-          acc_q[2] += 1.5 * dx * dz;
-          acc_q[3] += 1.5 * dy * dy - 0.5;
-          acc_q[4] += 1.5 * dy * dz;
-          acc_q[5] += 1.5 * dz * dz - 0.5;
-          acc_n[0] += dx;
-          acc_n[1] += dy;
-          acc_n[2] += dz;
-          if (((x + y + pb) & 1) == 0) {  // colour A: single-site terms (colour B added 2 bond + single above)
-            float sgl = 0.f;
-            const Vec3 v{vx, vy, vz};
-            if (GEO == GEO_SLAB) {
-              float sz;
-              const int sid = slab_surface(zw, nz, sz);
-              if (sid >= 0) sgl += anchoring_energy(m, sid, v, Vec3{0.f, 0.f, sz});
+          if (c.perx) {  // ghost columns: x + nx for x < 2, x - nx for x >= nx - 2
+            float *rowp = a.out + pbase + (long long)(yrows[iy] + GY) * R.px + GX;
+            for (int e = 0; e < 4; e++) {
+              const int x = xg + e;
+              if (x >= nx) break;
+              if (x < 2)
+#pragma unroll
+                for (int q = 0; q < 3; q++) rowp[q * R.comp + x + nx] = elem(v[q], e);
+              if (x >= nx - 2)
+#pragma unroll
+                for (int q = 0; q < 3; q++) rowp[q * R.comp + x - nx] = elem(v[q], e);
             }
-            if (m.field_on) sgl += field_energy(m, v, elecE);
-            acc_e += (double)sgl;
           }
+        }
+        if (measure) {
+          float f[kPartials];
+#pragma unroll
+          for (int q = 0; q < kPartials; q++) f[q] = 0.f;
+#pragma unroll
+          for (int e = 0; e < 4; e++) {
+            if (xg + e >= nx) continue;
+            const float vx = elem(v[0], e), vy = elem(v[1], e), vz = elem(v[2], e);
+            f[1] = fmaf(1.5f * vx, vx, f[1] - 0.5f);
+            f[2] = fmaf(1.5f * vx, vy, f[2]);
+            f[3] = fmaf(1.5f * vx, vz, f[3]);
+            f[4] = fmaf(1.5f * vy, vy, f[4] - 0.5f);
+            f[5] = fmaf(1.5f * vy, vz, f[5]);
+            f[6] = fmaf(1.5f * vz, vz, f[6] - 0.5f);
+            f[7] += vx;
+            f[8] += vy;
+            f[9] += vz;
+            if (((xg + e + y + kw) & 1) == 0 && (sid >= 0 || m.field_on))  // colour A: single-site terms
+              f[0] += single_energy(m, Vec3{vx, vy, vz}, sid, Vec3{0.f, 0.f, sz}, c.elecE);
+          }
+#pragma unroll
+          for (int q = 0; q < kPartials; q++) dacc[q] += (double)f[q];
         }
       }
     }
-    __syncthreads();  // slot of plane k - 2 is free after this step
   }
 
   if (!ok) {
-    // bail out: record the failure and wait (bounded) for this CTA's loads still in flight
     if (tid == 0) {
       atomicOr(a.err, 1u);
-      // loads possibly in flight: the last NSLOT issued planes (one per slot)
-      for (int p = max(pbeg, last_issued - NSLOT + 1); p <= last_issued; p++) {
+      for (int p = max(waited + 1, last_issued - NSL + 1); p <= last_issued; p++) {
         if (!plane_exists(p) || (a.skip_first_load && p == pbeg)) continue;
         const int lp = p - pbeg;
-        mbar_wait_bounded(&bars[lp % NSLOT], (unsigned)((lp / NSLOT) & 1), a.timeout_ns);
+        mbar_wait_bounded(&bars[lp % NSL], (unsigned)((lp / NSL) & 1), a.timeout_ns);
       }
     }
     __syncthreads();
     return;
   }
 
-  // reductions: acceptance count and the FP64 partials of this work item
   const unsigned wsum = __reduce_add_sync(0xffffffffu, accepted);
   if ((tid & 31) == 0 && wsum) atomicAdd(&a.st[it.rep].acc, (unsigned long long)wsum);
-  if (MEASURE) {
-    __shared__ double red[FT / 32][kPartials];
-    double v[kPartials] = {acc_e, acc_q[0], acc_q[1], acc_q[2], acc_q[3], acc_q[4], acc_q[5], acc_n[0], acc_n[1], acc_n[2]};
+  if (measure) {
+    __shared__ double red[NT / 32][kPartials];
     const int lane = tid & 31, warp = tid >> 5;
 #pragma unroll
-    for (int k = 0; k < kPartials; k++) {
-      double x = v[k];
+    for (int q = 0; q < kPartials; q++) {
+      double x = dacc[q];
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-      if (lane == 0) red[warp][k] = x;
+      if (lane == 0) red[warp][q] = x;
     }
     __syncthreads();
     if (tid < kPartials) {
       double x = 0.0;
-      for (int w = 0; w < FT / 32; w++) x += red[w][tid];
+      for (int w = 0; w < NT / 32; w++) x += red[w][tid];
       a.partials[(long long)blockIdx.x * kPartials + tid] = x;
     }
   }
@@ -446,7 +546,7 @@ bool fused_supported(const mcl_engine *e) {
 static int encode_map(CUtensorMap *map, float *base, const RepDesc &D, int tx, int ty) {
   cuuint64_t dims[4] = {(cuuint64_t)D.px, (cuuint64_t)D.py, (cuuint64_t)D.nz, 3};
   cuuint64_t strides[3] = {(cuuint64_t)D.px * 4, (cuuint64_t)D.px * D.py * 4, (cuuint64_t)D.comp * 4};
-  cuuint32_t box[4] = {(cuuint32_t)(tx + 8), (cuuint32_t)(ty + 4), 1, 3};
+  cuuint32_t box[4] = {(cuuint32_t)(tx + 8), (cuuint32_t)(ty + 4), 1, 3};  // one plane window, 16-byte rows
   cuuint32_t es[4] = {1, 1, 1, 1};
   CUresult r = get_encode()(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base + D.off, dims, strides, box, es,
                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -461,55 +561,60 @@ static int encode_map(CUtensorMap *map, float *base, const RepDesc &D, int tx, i
     if (e_ != cudaSuccess) return cuda_fail(e_, #call);  \
   } while (0)
 
-// Tile and segment choice: 64 x 16 tiles (x a multiple of 4 for the TMA box), and z segments sized so that the
-// number of work items is close to a multiple of the resident CTAs (2 per SM).
-static void choose_tiles(const mcl_engine *e, FusedPlan &P, int sms) {
-  P.tx = 64;
-  P.ty = 16;
+// Tile and segment choice for configuration `cfg`: z segments sized so that the number of work items is close to
+// a multiple of the resident CTAs, with segments long enough that the four extra planes of each stay cheap.
+static void choose_segments(const mcl_engine *e, FusedPlan &P, int sms) {
+  const FusedCfg &C = kCfgs[P.cfg];
+  P.tx = TXF;
+  P.ty = C.ty;
   long long tiles = 0, maxz = 1;
   for (auto &D : e->desc) {
     tiles += (long long)((D.nx + P.tx - 1) / P.tx) * ((D.ny + P.ty - 1) / P.ty);
     maxz = std::max<long long>(maxz, D.nz);
   }
-  const long long slots = 2ll * sms;
-  // smallest segment count (longest segments) whose item count fills the resident slots about evenly
+  const long long slots = (long long)C.ctas_per_sm * sms;
   int best = 1;
-  double best_eff = 0;
-  for (int nseg = 1; nseg <= 64; nseg++) {
-    long long items = tiles * nseg;
-    double waves = (double)items / slots;
-    double eff = waves / std::ceil(waves);
-    // extra planes per segment cost ~4/seg_len of the reads
-    double seg_len = (double)maxz / nseg;
-    if (seg_len < 8) break;
-    double score = eff * (1.0 - 4.0 / (seg_len + 4.0) * 0.5);
-    if (score > best_eff + 1e-9) {
-      best_eff = score;
+  double best_score = -1;
+  for (int nseg = 1; nseg <= 256; nseg++) {
+    const double seg_len = (double)maxz / nseg;
+    if (seg_len < 6 && nseg > 1) break;
+    const long long items = tiles * nseg;
+    const double waves = (double)items / slots;
+    const double eff = waves / std::ceil(waves);
+    const double score = eff * seg_len / (seg_len + 4.0 * 0.35);  // extra planes mostly hit L2
+    if (score > best_score + 1e-9) {
+      best_score = score;
       best = nseg;
     }
   }
   P.seg = (int)((maxz + best - 1) / best);
 }
 
-int fused_create(mcl_engine *e) {
-  FusedPlan *P = new FusedPlan();
-  e->fused = P;
+static int choose_cfg(const mcl_engine *e) {
+  // smaller lattices (few tiles) favour the 2-CTA configuration; large planes the 30-row tiles
+  long long area = 0;
+  for (auto &D : e->desc) area += (long long)D.nx * D.ny;
+  const char *env = getenv("MCL_FUSED_CFG");
+  if (env) return std::max(0, std::min(kNumCfgs - 1, atoi(env)));
+  return area >= 128ll * 128 ? 1 : 0;
+}
+
+static int build_items(mcl_engine *e, FusedPlan *P) {
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device);
-  choose_tiles(e, *P, sms);
-  // second director buffer
-  CKF(cudaMalloc(&e->d_dir[1], (size_t)e->dir_floats * sizeof(float)));
-  CKF(cudaMemsetAsync(e->d_dir[1], 0, (size_t)e->dir_floats * sizeof(float), e->stream));
-  // tensor maps
+  choose_segments(e, *P, sms);
   std::vector<CUtensorMap> maps(2 * e->n_rep);
   for (int r = 0; r < e->n_rep; r++)
     for (int b = 0; b < 2; b++) {
       int rc = encode_map(&maps[2 * r + b], e->d_dir[b], e->desc[r], P->tx, P->ty);
       if (rc) return rc;
     }
+  cudaFree(P->d_tmaps);
+  cudaFree(P->d_items);
+  cudaFree(P->d_first);
+  cudaFree(P->d_partials);
   CKF(cudaMalloc(&P->d_tmaps, maps.size() * sizeof(CUtensorMap)));
   CKF(cudaMemcpy(P->d_tmaps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice));
-  // work items, replica-major, then z segment, y tile, x tile
   std::vector<FusedItem> items;
   std::vector<int> first;
   for (int r = 0; r < e->n_rep; r++) {
@@ -526,10 +631,36 @@ int fused_create(mcl_engine *e) {
   CKF(cudaMalloc(&P->d_first, first.size() * sizeof(int)));
   CKF(cudaMemcpy(P->d_first, first.data(), first.size() * sizeof(int), cudaMemcpyHostToDevice));
   CKF(cudaMalloc(&P->d_partials, (size_t)P->n_items * kPartials * sizeof(double)));
+  const size_t slot_floats = ((size_t)3 * (P->tx + 8) * (P->ty + 4) + 31) / 32 * 32;
+  P->smem = 128 + (size_t)NSL * slot_floats * sizeof(float) + NSL * sizeof(unsigned long long);
+  return MCL_OK;
+}
+
+int fused_create(mcl_engine *e) {
+  FusedPlan *P = new FusedPlan();
+  e->fused = P;
+  P->cfg = choose_cfg(e);
+  CKF(cudaMalloc(&e->d_dir[1], (size_t)e->dir_floats * sizeof(float)));
+  CKF(cudaMemsetAsync(e->d_dir[1], 0, (size_t)e->dir_floats * sizeof(float), e->stream));
   CKF(cudaMalloc(&P->d_err, sizeof(unsigned int)));
   CKF(cudaMemset(P->d_err, 0, sizeof(unsigned int)));
-  const size_t slot_floats = ((size_t)3 * (P->tx + 8) * (P->ty + 4) + 31) / 32 * 32;
-  P->smem = 128 + (size_t)NSLOT * slot_floats * sizeof(float) + NSLOT * sizeof(unsigned long long);
+  return build_items(e, P);
+}
+
+int fused_set_cfg(mcl_engine *e, int cfg) {
+  if (!e->fused) return fail(MCL_ERR_STATE, "this engine does not use the fused tiled sweep");
+  if (cfg < 0 || cfg >= kNumCfgs) return fail(MCL_ERR_ARG, "tile configuration %d outside 0..%d", cfg, kNumCfgs - 1);
+  CKF(cudaStreamSynchronize(e->stream));
+  e->fused->cfg = cfg;
+  return build_items(e, e->fused);
+}
+
+int fused_get_cfg(const mcl_engine *e, int *cfg, int *ty, int *seg, int *items) {
+  if (!e->fused) return fail(MCL_ERR_STATE, "this engine does not use the fused tiled sweep");
+  if (cfg) *cfg = e->fused->cfg;
+  if (ty) *ty = e->fused->ty;
+  if (seg) *seg = e->fused->seg;
+  if (items) *items = e->fused->n_items;
   return MCL_OK;
 }
 
@@ -545,23 +676,32 @@ void fused_destroy(mcl_engine *e) {
   e->fused = nullptr;
 }
 
-template <int POT, int GEO, bool MEAS>
+template <int POT, int GEO, bool FLIP, int TY, int NT>
 static cudaError_t launch_one(const mcl_engine *e, const FusedArgs &a) {
-  auto k = k_sweep_fused<POT, GEO, MEAS>;
+  auto k = k_sweep_fused<POT, GEO, FLIP, TY, NT>;
   cudaError_t err = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e->fused->smem);
   if (err != cudaSuccess) return err;
-  k<<<e->fused->n_items, FT, e->fused->smem, e->stream>>>(e->model, a);
+  k<<<e->fused->n_items, NT, e->fused->smem, e->stream>>>(e->model, a);
   return cudaGetLastError();
 }
 
+template <int POT, int GEO, bool FLIP>
+static cudaError_t launch_cfg(const mcl_engine *e, const FusedArgs &a) {
+  switch (e->fused->cfg) {
+    case 1: return launch_one<POT, GEO, FLIP, 30, 512>(e, a);
+    default: return launch_one<POT, GEO, FLIP, 14, 256>(e, a);
+  }
+}
+
 template <int POT, int GEO>
-static cudaError_t launch_meas(const mcl_engine *e, const FusedArgs &a, bool measure) {
-  return measure ? launch_one<POT, GEO, true>(e, a) : launch_one<POT, GEO, false>(e, a);
+static cudaError_t launch_flip(const mcl_engine *e, const FusedArgs &a) {
+  if (POT == POT_PEAR) return launch_cfg<POT, GEO, true>(e, a);
+  return e->model.flip ? launch_cfg<POT, GEO, true>(e, a) : launch_cfg<POT, GEO, false>(e, a);
 }
 
 template <int POT>
-static cudaError_t launch_geo(const mcl_engine *e, const FusedArgs &a, bool measure) {
-  return e->geo == GEO_SLAB ? launch_meas<POT, GEO_SLAB>(e, a, measure) : launch_meas<POT, GEO_BULK>(e, a, measure);
+static cudaError_t launch_geo(const mcl_engine *e, const FusedArgs &a) {
+  return e->geo == GEO_SLAB ? launch_flip<POT, GEO_SLAB>(e, a) : launch_flip<POT, GEO_BULK>(e, a);
 }
 
 int fused_sweep(mcl_engine *e, bool measure, cudaEvent_t ev0, cudaEvent_t ev1) {
@@ -576,18 +716,17 @@ int fused_sweep(mcl_engine *e, bool measure, cudaEvent_t ev0, cudaEvent_t ev1) {
   a.sweep_ctr = e->d_sweep;
   a.err = P->d_err;
   a.cur = e->cur;
-  a.tx = P->tx;
-  a.ty = P->ty;
+  a.measure = measure ? 1 : 0;
   a.timeout_ns = P->timeout_ns;
   a.skip_first_load = P->skip_first_load;
   if (ev0) CKF(cudaEventRecord(ev0, e->stream));
   cudaError_t err;
   if (e->model.potential == POT_GHRL)
-    err = launch_geo<POT_GHRL>(e, a, measure);
+    err = launch_geo<POT_GHRL>(e, a);
   else if (e->model.potential == POT_PEAR)
-    err = launch_geo<POT_PEAR>(e, a, measure);
+    err = launch_geo<POT_PEAR>(e, a);
   else
-    err = launch_geo<POT_LL>(e, a, measure);
+    err = launch_geo<POT_LL>(e, a);
   if (err != cudaSuccess) return cuda_fail(err, "fused sweep launch");
   if (ev1) CKF(cudaEventRecord(ev1, e->stream));
   e->cur ^= 1;

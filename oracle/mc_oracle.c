@@ -36,12 +36,26 @@ void mco_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t ou
   out[3] = c3;
 }
 
-void mco_site_uniforms(uint64_t seed, uint64_t sweep, uint32_t site, uint32_t stream, double u[4]) {
-  uint32_t ctr[4] = {site, (uint32_t)sweep, (uint32_t)(sweep >> 32), stream};
+void mco_site_uniforms(uint64_t seed, uint64_t sweep, int x, int y, int z, int nx, int ny, int flip, double u[4]) {
   uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
-  uint32_t x[4];
-  mco_philox4x32_10(ctr, key, x);
-  for (int k = 0; k < 4; k++) u[k] = (double)(x[k] >> 8) * (1.0 / 16777216.0);
+  uint32_t o[4];
+  if (flip) {
+    uint32_t ctr[4] = {(uint32_t)x + (uint32_t)nx * ((uint32_t)y + (uint32_t)ny * (uint32_t)z), (uint32_t)sweep,
+                       (uint32_t)(sweep >> 32), 0};
+    mco_philox4x32_10(ctr, key, o);
+    for (int k = 0; k < 4; k++) u[k] = (double)(o[k] >> 8) * (1.0 / 16777216.0);
+    return;
+  }
+  uint32_t ctr[4] = {((uint32_t)x & ~2u) + (uint32_t)nx * ((uint32_t)y + (uint32_t)ny * (uint32_t)z), (uint32_t)sweep,
+                     (uint32_t)(sweep >> 32), 0};
+  mco_philox4x32_10(ctr, key, o);
+  const int h = (x >> 1) & 1;
+  const uint32_t lo = o[2 * h], hi = o[2 * h + 1];
+  const double s21 = 1.0 / 2097152.0;
+  u[0] = (double)(lo & 0x1FFFFFu) * s21;
+  u[1] = (double)(((lo >> 21) | (hi << 11)) & 0x1FFFFFu) * s21;
+  u[2] = (double)((hi >> 10) & 0x1FFFFFu) * s21;
+  u[3] = 0;
 }
 
 /* ------------------------------------------------------------------------------------------------ */
@@ -273,7 +287,8 @@ double mco_site_energy_fp64(const mco_model *m, const mco_lattice *L, const floa
 static int update_site(const mco_model *m, const mco_lattice *L, float *ni, int idx, float T, float ang_var,
                        uint64_t seed, uint64_t sweep, uint8_t *decisions, float *margin) {
   double u[4];
-  mco_site_uniforms(seed, sweep, (uint32_t)idx, 0, u);
+  const int x = idx % L->nx, y = (idx / L->nx) % L->ny, z = idx / (L->nx * L->ny);
+  mco_site_uniforms(seed, sweep, x, y, z, L->nx, L->ny, m->flip_move, u);
   float *n = &ni[3 * idx];
   float va = (float)((2 * u[0] - 1) * (double)ang_var);
   float rotation_type = (float)u[1];
@@ -412,7 +427,7 @@ int64_t mco_ref8_stream(const mco_model *m, const mco_lattice *L, uint64_t seed,
       int idx = i + Nx * (j + Ny * k);
       if (!pt_of(L, idx)) continue;
       double u[4];
-      mco_site_uniforms(seed, sweep, (uint32_t)idx, 0, u);
+      mco_site_uniforms(seed, sweep, i, j, k, Nx, Ny, m->flip_move, u);
       int n = m->flip_move ? 4 : 3;
       for (int q = 0; q < n; q++) {
         if (w < cap) out[w] = u[q];

@@ -56,8 +56,14 @@ typedef struct mco_lattice {
 
 /* Philox4x32-10 block function. */
 void mco_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
-/* The four uniforms (multiples of 2^-24 in [0,1)) of `site` in `sweep` for the plain move. */
-void mco_site_uniforms(uint64_t seed, uint64_t sweep, uint32_t site, uint32_t stream, double u[4]);
+/* The uniforms of site (x, y, z) in `sweep` for the plain move: u[0] angle, u[1] axis, u[2] rotation
+ * acceptance, u[3] flip acceptance.
+ *  flip models (flip != 0): one Philox call per site, counter (site, sweep lo, sweep hi, 0), u[k] = (out[k] >> 8)
+ *    2^-24;
+ *  other models: one call per pair of same-colour sites x and x ^ 2 of a row, counter (linear index of
+ *    (x & ~2, y, z), sweep lo, sweep hi, 0); the site uses the 64-bit half h = (x >> 1) & 1 of the output, split
+ *    into three 21-bit fields: u = field 2^-21; u[3] = 0. */
+void mco_site_uniforms(uint64_t seed, uint64_t sweep, int x, int y, int z, int nx, int ny, int flip, double u[4]);
 
 /* Site energy of site idx with its director replaced by n (reference geometry*::site_energy). */
 float mco_site_energy(const mco_model *m, const mco_lattice *L, const float *ni, int idx, const float n[3]);

@@ -47,8 +47,8 @@ def lib():
         L = ctypes.CDLL(path)
         P = ctypes.POINTER
         L.mco_philox4x32_10.argtypes = [P(ctypes.c_uint32), P(ctypes.c_uint32), P(ctypes.c_uint32)]
-        L.mco_site_uniforms.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32,
-                                        P(ctypes.c_double)]
+        L.mco_site_uniforms.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_int, ctypes.c_int, ctypes.c_int, P(ctypes.c_double)]
         L.mco_site_energy.argtypes = [P(Model), P(Lattice), ctypes.c_void_p, ctypes.c_int, P(ctypes.c_float)]
         L.mco_site_energy.restype = ctypes.c_float
         L.mco_sweep.argtypes = [P(Model), P(Lattice), ctypes.c_void_p, ctypes.c_float, P(ctypes.c_float),
@@ -77,9 +77,9 @@ def philox(ctr, key):
     return list(o)
 
 
-def site_uniforms(seed, sweep, site, stream=0):
+def site_uniforms(seed, sweep, x, y, z, nx, ny, flip):
     u = (ctypes.c_double * 4)()
-    lib().mco_site_uniforms(seed, sweep, site, stream, u)
+    lib().mco_site_uniforms(seed, sweep, x, y, z, nx, ny, flip, u)
     return list(u)
 
 
