@@ -1,17 +1,19 @@
 // Shared device-side definitions: lattice layout, replica descriptors, model constants and the counter-based RNG.
 //
-// Director storage in HBM (per replica, per buffer): three FP32 component planes-of-planes (SoA),
-//   dir[off + (c * nz + z) * py * px + (y + GY) * px + (x + GX)],   c = 0, 1, 2 (x, y, z component),
-// with px = round_up(nx, 4) + 2 GX and py = ny + 2 GY. The rows carry GX = 4 cells of padding on each side and
-// the planes GY = 2 rows, so that a TMA box starting 4 cells left of a 4-aligned tile stays 16-byte aligned.
-// For a periodic axis the two cells next to each edge (x = -2, -1, nx, nx+1; likewise y) hold copies of the
+// Director storage in HBM (per replica, per buffer): three FP32 component volumes (SoA). Every row of a plane is
+// stored split by x parity: the even-x sites first, then the odd-x sites, each half-row padded by GH = 4 cells on
+// the left and at least 4 on the right:
+//   dir[off + (c * nz + z) * py * px + (y + GY) * px + (x & 1) * hp + (x >> 1) + GH],
+// hp = round_up(ceil(nx / 2), 4) + 8, px = 2 hp, py = ny + 2 GY, GY = 2. One colour of the checkerboard in a row is
+// thus one contiguous half-row, and a 16-byte aligned TMA box can start 4 cells left of any tile that begins at a
+// multiple of 8 in x. For a periodic axis the cells x = -2, -1, nx, nx + 1 (likewise y) hold copies of the
 // wrapped sites ("ghosts"); the fused kernel reads them instead of wrapping. Padding beyond is zero.
 #pragma once
 #include <stdint.h>
 
 namespace mcl {
 
-constexpr int GX = 4;
+constexpr int GH = 4;  // left padding of a half-row
 constexpr int GY = 2;
 constexpr int kMaxSurfaces = 16;
 
@@ -45,10 +47,10 @@ struct ModelDev {
 // Immutable per-replica layout.
 struct RepDesc {
   int nx, ny, nz;
-  int px, py;
+  int px, py;        // row pitch (2 hp) and padded rows per plane
   int geo;           // Geo
   int periodic[3];
-  int pad0;
+  int hp;            // half-row pitch
   long long off;     // float offset of this replica in the director buffers
   long long comp;    // floats per component = nz * py * px
   long long site_off;  // offset of this replica in the unpadded per-site arrays (pt, normals, decisions)
@@ -71,7 +73,7 @@ struct ObsRecord {
 constexpr int kPartials = 10;
 
 __host__ __device__ inline long long dir_index(const RepDesc &r, int c, int x, int y, int z) {
-  return r.off + (long long)c * r.comp + ((long long)z * r.py + (y + GY)) * r.px + (x + GX);
+  return r.off + (long long)c * r.comp + ((long long)z * r.py + (y + GY)) * r.px + (x & 1) * r.hp + (x >> 1) + GH;
 }
 
 // ---- Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11) ------------------------------------------------------

@@ -230,7 +230,8 @@ int mcl_create(const mcl_model *model, const mcl_replica *replicas, int n_replic
     D.nx = R.nx;
     D.ny = R.ny;
     D.nz = R.nz;
-    D.px = ((R.nx + 3) / 4) * 4 + 2 * GX;
+    D.hp = (((R.nx + 1) / 2 + 3) / 4) * 4 + 2 * GH;
+    D.px = 2 * D.hp;
     D.py = R.ny + 2 * GY;
     D.geo = geo_class;
     D.periodic[0] = R.periodic[0] != 0;

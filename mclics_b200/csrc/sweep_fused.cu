@@ -59,7 +59,7 @@ struct FusedArgs {
 struct FusedCfg {
   int ty, nt, ctas_per_sm;
 };
-static const FusedCfg kCfgs[] = {{14, 256, 2}, {30, 512, 1}};
+static const FusedCfg kCfgs[] = {{14, 256, 2}, {28, 512, 1}};
 constexpr int kNumCfgs = 2;
 
 struct FusedPlan {
@@ -106,12 +106,12 @@ __device__ __forceinline__ unsigned long long globaltimer() {
   return t;
 }
 
-__device__ __forceinline__ void tma_load_plane(float *dst, const CUtensorMap *map, int x, int y, int z,
+__device__ __forceinline__ void tma_load_plane(float *dst, const CUtensorMap *map, int j, int y, int z,
                                                unsigned long long *bar) {
   asm volatile(
-      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
-      "[%6];" ::"r"(smem_u32(dst)),
-      "l"(map), "r"(x), "r"(y), "r"(z), "r"(0), "r"(smem_u32(bar))
+      "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], "
+      "[%7];" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(j), "r"(0), "r"(y), "r"(z), "r"(0), "r"(smem_u32(bar))
       : "memory");
 }
 
@@ -126,23 +126,18 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, unsig
 }
 
 // ---- the kernel --------------------------------------------------------------------------------------------
-// Tile: TX = 64 columns (16 groups of 4 cells) x TY rows. Window in shared memory: W = TX + 8 columns (x0 - 4 ..
-// x0 + TX + 3) by H = TY + 4 rows (y0 - 2 .. y0 + TY + 1), three component planes, one TMA box per slot.
-constexpr int TXF = 64, NG = TXF / 4, WF = TXF + 8, NSL = 7;
+// Tile: TX = 64 columns (32 sites of each x parity) x TY rows. Window in shared memory, per component and row:
+// the even-x half-row then the odd-x half-row, 40 cells each (half-row index j0 - 4 .. j0 + 35, j0 = x0 / 2), for
+// rows y0 - 2 .. y0 + TY + 1: exactly one 5-D TMA box (40, 2, TY + 4, 1, 3) of the split HBM layout.
+constexpr int TXF = 64, HALF = 40, RW = 2 * HALF, NPAIR = 16, NSL = 7;
 
 template <int TY>
 struct Win {
-  static constexpr int W = WF, H = TY + 4, PF = W * H, SLOT = (3 * PF + 31) / 32 * 32;
+  static constexpr int H = TY + 4, PF = RW * H, SLOT = (3 * PF + 31) / 32 * 32;
 };
 
-__device__ __forceinline__ float elem(const float4 &v, int e) {  // e is a compile-time constant at every call
+__device__ __forceinline__ float f4get(const float4 &v, int e) {  // e compile-time after unrolling
   return e == 0 ? v.x : (e == 1 ? v.y : (e == 2 ? v.z : v.w));
-}
-__device__ __forceinline__ void set_elem(float4 &v, int e, float x) {
-  if (e == 0) v.x = x;
-  else if (e == 1) v.y = x;
-  else if (e == 2) v.z = x;
-  else v.w = x;
 }
 
 // Geometry/boundary facts of a work item that the site updates need.
@@ -153,32 +148,32 @@ struct Ctx {
   float T, invT, av, elecE;
 };
 
-// One task: the two sites (xg + E, y) and (xg + E + 2, y) of one colour in the 4-cell group starting at window
-// column wc (= xg - x0 + 4) of window row wy. v0 / v1: whether each site is to be updated. Returns the updated
-// group back into shared memory; adds the accepted rotations of counted sites and (bond, single) of measured sites.
-template <int POT, int GEO, bool FLIP, int TY, int E>
+// One task: the two sites of half-row h (x parity h) at window half-row cells jb and jb + 1 (jb even), i.e. sites
+// x = 2 (j0 - 4 + jb) + h and x + 2 of row y. v0 / v1: whether each is updated. The updated pair goes back to shared
+// memory; accepted rotations of counted sites and (2 bond + single) of measured sites are accumulated.
+template <int POT, int GEO, bool FLIP, int TY>
 __device__ __forceinline__ void pair_task(const ModelDev &m, const Ctx &c, float *cs, const float *below,
-                                          const float *above, int wy, int wc, int xg, int y, int zw, bool v0, bool v1,
-                                          bool count, bool meas_b, unsigned &accepted, float &e_acc) {
-  constexpr int W = Win<TY>::W, PF = Win<TY>::PF;
-  float *row = cs + wy * W + wc;
-  float4 o[3], yu[3], yd[3], zu[3], zd[3];
-  float ex[3];
+                                          const float *above, int wy, int h, int jb, int x, int y, int zw, bool v0,
+                                          bool v1, bool count, bool meas, unsigned &accepted, float &e_acc) {
+  constexpr int PF = Win<TY>::PF;
+  float *own = cs + (wy * 2 + h) * HALF + jb;                 // component 0
+  const float *oth = cs + (wy * 2 + (h ^ 1)) * HALF + jb - 1 + h;  // other parity, 3 consecutive cells
+  const int up = 2 * HALF, dn = -2 * HALF;                    // same half-row of the next / previous row
+  const float *zu = above ? above + (wy * 2 + h) * HALF + jb : own;
+  const float *zd = below ? below + (wy * 2 + h) * HALF + jb : own;
+  float2 o[3], yu[3], yd[3], pu[3], pd[3];
+  float xa[3], xb[3], xc[3];
 #pragma unroll
   for (int q = 0; q < 3; q++) {
-    o[q] = *reinterpret_cast<const float4 *>(row + q * PF);
-    yu[q] = *reinterpret_cast<const float4 *>(row + q * PF + W);
-    yd[q] = *reinterpret_cast<const float4 *>(row + q * PF - W);
-    ex[q] = E == 0 ? row[q * PF - 1] : row[q * PF + 4];
+    o[q] = *reinterpret_cast<const float2 *>(own + q * PF);
+    yu[q] = *reinterpret_cast<const float2 *>(own + q * PF + up);
+    yd[q] = *reinterpret_cast<const float2 *>(own + q * PF + dn);
+    pu[q] = *reinterpret_cast<const float2 *>(zu + q * PF);
+    pd[q] = *reinterpret_cast<const float2 *>(zd + q * PF);
+    xa[q] = oth[q * PF];
+    xb[q] = oth[q * PF + 1];
+    xc[q] = oth[q * PF + 2];
   }
-  const float wz_up = above ? 1.f : 0.f, wz_dn = below ? 1.f : 0.f;
-  const float *rowu = above ? above + wy * W + wc : row, *rowd = below ? below + wy * W + wc : row;
-#pragma unroll
-  for (int q = 0; q < 3; q++) {
-    zu[q] = *reinterpret_cast<const float4 *>(rowu + q * PF);
-    zd[q] = *reinterpret_cast<const float4 *>(rowd + q * PF);
-  }
-  // surface of this plane (slab): uniform per plane
   int sid = -1;
   Vec3 sn{0.f, 0.f, 0.f};
   if (GEO == GEO_SLAB) {
@@ -188,60 +183,47 @@ __device__ __forceinline__ void pair_task(const ModelDev &m, const Ctx &c, float
   }
   const int yw = c.pery ? (y < 0 ? y + c.ny : (y >= c.ny ? y - c.ny : y)) : y;
   const float wyp = (c.pery || y + 1 < c.ny) ? 1.f : 0.f, wym = (c.pery || y - 1 >= 0) ? 1.f : 0.f;
-  SiteResult r[2];
-  Draw d[2];
-  int xs[2] = {xg + E, xg + E + 2};
+  const float wzu = above ? 1.f : 0.f, wzd = below ? 1.f : 0.f;
+  const int xs[2] = {x, x + 2};
   int xw[2];
 #pragma unroll
   for (int s = 0; s < 2; s++) xw[s] = c.perx ? (xs[s] < 0 ? xs[s] + c.nx : (xs[s] >= c.nx ? xs[s] - c.nx : xs[s])) : xs[s];
+  Draw d[2];
   if (FLIP) {
 #pragma unroll
     for (int s = 0; s < 2; s++) d[s] = site_draw(c.seed, c.sweep, xw[s], yw, zw, c.nx, c.ny, true);
   } else {
-    // one Philox call for the pair: both sites share x & ~2 unless a periodic wrap split them (ring columns)
-    const int sv = v0 ? 0 : 1;
-    const U4 out = site_draws(c.seed, c.sweep, pair_counter(xw[sv], yw, zw, c.nx, c.ny), 0);
+    // one Philox call serves both sites (x & ~2 is shared) unless a periodic wrap split a ring pair
+    const U4 out = site_draws(c.seed, c.sweep, pair_counter(xw[v0 ? 0 : 1], yw, zw, c.nx, c.ny), 0);
     d[0] = pair_half(out, (xw[0] >> 1) & 1u);
     d[1] = pair_half(out, (xw[1] >> 1) & 1u);
   }
+  SiteResult r[2];
 #pragma unroll
   for (int s = 0; s < 2; s++) {
-    const int e = E + 2 * s;  // element of the site in the group
-    const Vec3 n{elem(o[0], e), elem(o[1], e), elem(o[2], e)};
+    const Vec3 n = s == 0 ? Vec3{o[0].x, o[1].x, o[2].x} : Vec3{o[0].y, o[1].y, o[2].y};
     Vec3 nb[6];
-    // +x: element e+1 (or the extra cell for E = 1, s = 1); -x: element e-1 (or the extra cell for E = 0, s = 0)
-    if (e + 1 <= 3)
-      nb[0] = Vec3{elem(o[0], e + 1), elem(o[1], e + 1), elem(o[2], e + 1)};
-    else
-      nb[0] = Vec3{ex[0], ex[1], ex[2]};
-    if (e - 1 >= 0)
-      nb[1] = Vec3{elem(o[0], e - 1), elem(o[1], e - 1), elem(o[2], e - 1)};
-    else
-      nb[1] = Vec3{ex[0], ex[1], ex[2]};
-    nb[2] = Vec3{elem(yu[0], e), elem(yu[1], e), elem(yu[2], e)};
-    nb[3] = Vec3{elem(yd[0], e), elem(yd[1], e), elem(yd[2], e)};
-    nb[4] = Vec3{elem(zu[0], e), elem(zu[1], e), elem(zu[2], e)};
-    nb[5] = Vec3{elem(zd[0], e), elem(zd[1], e), elem(zd[2], e)};
-    const float w[6] = {(c.perx || xs[s] + 1 < c.nx) ? 1.f : 0.f, (c.perx || xs[s] - 1 >= 0) ? 1.f : 0.f, wyp, wym,
-                        wz_up, wz_dn};
+    nb[0] = s == 0 ? Vec3{xb[0], xb[1], xb[2]} : Vec3{xc[0], xc[1], xc[2]};  // +x
+    nb[1] = s == 0 ? Vec3{xa[0], xa[1], xa[2]} : Vec3{xb[0], xb[1], xb[2]};  // -x
+    nb[2] = s == 0 ? Vec3{yu[0].x, yu[1].x, yu[2].x} : Vec3{yu[0].y, yu[1].y, yu[2].y};
+    nb[3] = s == 0 ? Vec3{yd[0].x, yd[1].x, yd[2].x} : Vec3{yd[0].y, yd[1].y, yd[2].y};
+    nb[4] = s == 0 ? Vec3{pu[0].x, pu[1].x, pu[2].x} : Vec3{pu[0].y, pu[1].y, pu[2].y};
+    nb[5] = s == 0 ? Vec3{pd[0].x, pd[1].x, pd[2].x} : Vec3{pd[0].y, pd[1].y, pd[2].y};
+    const float w[6] = {(c.perx || xs[s] + 1 < c.nx) ? 1.f : 0.f, (c.perx || xs[s] - 1 >= 0) ? 1.f : 0.f, wyp, wym, wzu,
+                        wzd};
     r[s] = site_update<POT, FLIP>(m, n, nb, w, sid, sn, c.elecE, d[s], c.av, c.T, c.invT);
   }
   if (v0 | v1) {
-    if (v0) {
-      set_elem(o[0], E, r[0].n.x);
-      set_elem(o[1], E, r[0].n.y);
-      set_elem(o[2], E, r[0].n.z);
-    }
-    if (v1) {
-      set_elem(o[0], E + 2, r[1].n.x);
-      set_elem(o[1], E + 2, r[1].n.y);
-      set_elem(o[2], E + 2, r[1].n.z);
-    }
 #pragma unroll
-    for (int q = 0; q < 3; q++) *reinterpret_cast<float4 *>(row + q * PF) = o[q];
+    for (int q = 0; q < 3; q++) {
+      float2 v = o[q];
+      if (v0) v.x = q == 0 ? r[0].n.x : (q == 1 ? r[0].n.y : r[0].n.z);
+      if (v1) v.y = q == 0 ? r[1].n.x : (q == 1 ? r[1].n.y : r[1].n.z);
+      *reinterpret_cast<float2 *>(own + q * PF) = v;
+    }
   }
   if (count) accepted += (v0 ? r[0].rot : 0u) + (v1 ? r[1].rot : 0u);
-  if (meas_b) {
+  if (meas) {
     if (v0) e_acc += fmaf(2.f, r[0].bond, r[0].single);
     if (v1) e_acc += fmaf(2.f, r[1].bond, r[1].single);
   }
@@ -249,7 +231,7 @@ __device__ __forceinline__ void pair_task(const ModelDev &m, const Ctx &c, float
 
 template <int POT, int GEO, bool FLIP, int TY, int NT>
 __global__ void __launch_bounds__(NT, NT <= 256 ? 2 : 1) k_sweep_fused(ModelDev m, FusedArgs a) {
-  constexpr int W = Win<TY>::W, PF = Win<TY>::PF, SLOT = Win<TY>::SLOT;
+  constexpr int PF = Win<TY>::PF, SLOT = Win<TY>::SLOT, H = Win<TY>::H;
   extern __shared__ __align__(128) unsigned char smem_dyn[];
   unsigned char *smem_raw = (unsigned char *)(((uintptr_t)smem_dyn + 127) & ~(uintptr_t)127);
   float *slots = reinterpret_cast<float *>(smem_raw);
@@ -263,6 +245,7 @@ __global__ void __launch_bounds__(NT, NT <= 256 ? 2 : 1) k_sweep_fused(ModelDev 
   const int nx = R.nx, ny = R.ny, nz = R.nz;
   const bool perz = R.periodic[2];
   const int x0 = it.x0, y0 = it.y0, z0 = it.z0, z1 = it.z1;
+  const int j0 = x0 >> 1;
   const bool measure = a.measure != 0;
   Ctx c;
   c.nx = nx;
@@ -303,7 +286,7 @@ __global__ void __launch_bounds__(NT, NT <= 256 ? 2 : 1) k_sweep_fused(ModelDev 
       return;
     }
     mbar_expect_tx(bar, box_bytes);
-    tma_load_plane(slot_ptr(p), map, x0, y0, wrapz(p), bar);
+    tma_load_plane(slot_ptr(p), map, j0, y0, wrapz(p), bar);
   };
   int waited = pbeg - 1;  // uniform: highest plane waited for successfully
   auto wait_plane = [&](int p) -> bool {
@@ -326,11 +309,11 @@ __global__ void __launch_bounds__(NT, NT <= 256 ? 2 : 1) k_sweep_fused(ModelDev 
 #pragma unroll
   for (int q = 0; q < kPartials; q++) dacc[q] = 0.0;
 
-  // ring column limits (colour A of owned planes): left x0 - 1, right min(x0 + TX, nx) (periodic) / x0 + TX
+  // ring columns (colour A of owned planes): left x0 - 1, right min(x0 + TX, nx) (periodic) / x0 + TX (free)
   const bool has_left = c.perx || x0 >= 1;
   const int xright = c.perx ? min(x0 + TXF, nx) : x0 + TXF;
   const bool has_right = xright < nx || (c.perx && xright == nx);
-  const int ylim_ring = c.pery ? ny : ny - 1;  // highest valid ring row
+  const int ylo_ring = c.pery ? -1 : 0, yhi_ring = c.pery ? ny : ny - 1;
 
   bool ok = wait_plane(z0 - 2) && wait_plane(z0 - 1);
   for (int k = z0 - 1; ok && k <= z1 + 2; k++) {
@@ -344,9 +327,9 @@ __global__ void __launch_bounds__(NT, NT <= 256 ? 2 : 1) k_sweep_fused(ModelDev 
     const bool doB = kb >= z0 && kb < z1 && plane_exists(kb);
     const int rowsA = doA ? (ownA ? TY + 2 : TY) : 0;
     const int row0A = ownA ? y0 - 1 : y0;
-    const int nAg = rowsA * NG;
+    const int nAg = rowsA * NPAIR;
     const int nAc = (doA && ownA) ? TY : 0;  // TY/2 ring sites on each side
-    const int nB = doB ? TY * NG : 0;
+    const int nB = doB ? TY * NPAIR : 0;
     const int ntask = nAg + nAc + nB;
     const int zwA = wrapz(k), zwB = wrapz(kb);
     float *csA = doA ? slot_ptr(k) : nullptr;
@@ -357,62 +340,64 @@ __global__ void __launch_bounds__(NT, NT <= 256 ? 2 : 1) k_sweep_fused(ModelDev 
     const float *aboveB = (doB && plane_exists(kb + 1)) ? slot_ptr(kb + 1) : nullptr;
     float eB = 0.f;
     for (int t = tid; t < ntask; t += NT) {
+      float *cs;
+      const float *below, *above;
+      int y, x, h, jb, zw;
+      bool v0, v1, count, meas;
       if (t < nAg) {
-        // rows in parity order (even-offset rows first) so that warps see one element offset E
-        const int half_rows = (rowsA + 1) / 2;
-        const int rr = t / NG, g = t % NG;
-        const int ri = rr < half_rows ? 2 * rr : 2 * (rr - half_rows) + 1;
-        const int y = row0A + ri;
-        const int xg = x0 + 4 * g;
-        const bool yok = ownA ? (y >= (c.pery ? -1 : 0) && y <= ylim_ring && !(y >= ny && y != ny)) : (y < ny);
-        const bool yint = y >= y0 && y < y0 + TY && y < ny;
-        const int E = (y + k) & 1;  // colour A: x + y + k even, xg is a multiple of 4
-        const bool v0 = yok && xg + E < nx, v1 = yok && xg + E + 2 < nx;
-        const int wy = y - y0 + 2, wc = xg - x0 + 4;
-        if (E == 0)
-          pair_task<POT, GEO, FLIP, TY, 0>(m, c, csA, belowA, aboveA, wy, wc, xg, y, zwA, v0, v1, ownA && yint, false,
-                                           accepted, eB);
-        else
-          pair_task<POT, GEO, FLIP, TY, 1>(m, c, csA, belowA, aboveA, wy, wc, xg, y, zwA, v0, v1, ownA && yint, false,
-                                           accepted, eB);
+        const int rr = t / NPAIR, p = t % NPAIR;
+        y = row0A + rr;
+        h = (y + k) & 1;  // colour A: x + y + k even
+        jb = 4 + 2 * p;
+        x = x0 + 4 * p + h;
+        const bool yok = ownA ? (y >= ylo_ring && y <= yhi_ring) : (y < ny);
+        v0 = yok && x < nx;
+        v1 = yok && x + 2 < nx;
+        cs = csA;
+        below = belowA;
+        above = aboveA;
+        zw = zwA;
+        count = ownA && y >= y0 && y < y0 + TY && y < ny;
+        meas = false;
       } else if (t < nAg + nAc) {
-        // ring columns: one site each, left side first
-        const int q = t - nAg, side = q / (TY / 2), j = q % (TY / 2);
-        const int xc = side == 0 ? x0 - 1 : xright;
-        const int y = y0 + 2 * j + ((xc + y0 + k) & 1);  // (xc + y + k) even
+        // ring columns, one site each (left side first)
+        const int q = t - nAg, side = q / (TY / 2), jr = q % (TY / 2);
+        const int xcol = side == 0 ? x0 - 1 : xright;
+        y = y0 + 2 * jr + ((xcol + y0 + k) & 1);  // (xcol + y + k) even
         const bool valid = (side == 0 ? has_left : has_right) && y < y0 + TY && y < ny;
-        const int xg = xc & ~3;  // floor to the group (xc may be -1)
-        const int e = xc - xg;
-        const int E = e & 1;
-        const int wy = y - y0 + 2, wc = xg - x0 + 4;
-        const bool v0 = valid && e == E, v1 = valid && e == E + 2;
-        if (E == 0)
-          pair_task<POT, GEO, FLIP, TY, 0>(m, c, csA, belowA, aboveA, wy, wc, xg, y, zwA, v0, v1, false, false,
-                                           accepted, eB);
-        else
-          pair_task<POT, GEO, FLIP, TY, 1>(m, c, csA, belowA, aboveA, wy, wc, xg, y, zwA, v0, v1, false, false,
-                                           accepted, eB);
+        h = xcol & 1;
+        const int jj = (xcol >> 1) - j0 + 4;  // window cell of the site
+        jb = jj & ~1;
+        x = xcol - 2 * (jj & 1);  // x of the pair's first site
+        v0 = valid && (jj & 1) == 0;
+        v1 = valid && (jj & 1) == 1;
+        cs = csA;
+        below = belowA;
+        above = aboveA;
+        zw = zwA;
+        count = false;
+        meas = false;
       } else {
         const int tb = t - nAg - nAc;
-        const int half_rows = (TY + 1) / 2;
-        const int rr = tb / NG, g = tb % NG;
-        const int ri = rr < half_rows ? 2 * rr : 2 * (rr - half_rows) + 1;
-        const int y = y0 + ri;
-        const int xg = x0 + 4 * g;
-        const int E = (y + kb + 1) & 1;  // colour B: x + y + kb odd
-        const bool yok = y < ny;
-        const bool v0 = yok && xg + E < nx, v1 = yok && xg + E + 2 < nx;
-        const int wy = y - y0 + 2, wc = xg - x0 + 4;
-        if (E == 0)
-          pair_task<POT, GEO, FLIP, TY, 0>(m, c, csB, belowB, aboveB, wy, wc, xg, y, zwB, v0, v1, true, measure,
-                                           accepted, eB);
-        else
-          pair_task<POT, GEO, FLIP, TY, 1>(m, c, csB, belowB, aboveB, wy, wc, xg, y, zwB, v0, v1, true, measure,
-                                           accepted, eB);
+        const int rr = tb / NPAIR, p = tb % NPAIR;
+        y = y0 + rr;
+        h = (y + kb + 1) & 1;  // colour B: x + y + kb odd
+        jb = 4 + 2 * p;
+        x = x0 + 4 * p + h;
+        v0 = y < ny && x < nx;
+        v1 = y < ny && x + 2 < nx;
+        cs = csB;
+        below = belowB;
+        above = aboveB;
+        zw = zwB;
+        count = true;
+        meas = measure;
       }
+      pair_task<POT, GEO, FLIP, TY>(m, c, cs, below, above, y - y0 + 2, h, jb, x, y, zw, v0, v1, count, meas, accepted,
+                                    eB);
     }
     if (measure) dacc[0] += (double)eB;
-    // ---- write-out of plane k - 3 (both colours final) and its site terms
+    // ---- write-out of plane k - 3 (both colours final): rows x halves x 8 chunks of 4 cells
     const int kw = k - 3;
     if (kw >= z0 && kw < z1 && plane_exists(kw)) {
       const float *cw = slot_ptr(kw);
@@ -421,53 +406,55 @@ __global__ void __launch_bounds__(NT, NT <= 256 ? 2 : 1) k_sweep_fused(ModelDev 
       int sid = -1;
       float sz = 0.f;
       if (GEO == GEO_SLAB) sid = slab_surface(zw, nz, sz);
-      for (int t = tid; t < TY * NG; t += NT) {
-        const int rr = t / NG, g = t % NG;
-        const int y = y0 + rr, xg = x0 + 4 * g;
-        if (y >= ny || xg >= nx) continue;
-        const int wy = rr + 2, wc = 4 * g + 4;
+      for (int t = tid; t < TY * 16; t += NT) {
+        const int rr = t >> 4, h = (t >> 3) & 1, q4 = t & 7;
+        const int y = y0 + rr;
+        const int jl = j0 + 4 * q4;  // first half-row index of the chunk
+        const int xfirst = 2 * jl + h;
+        if (y >= ny || xfirst >= nx) continue;
+        const int cell = ((rr + 2) * 2 + h) * HALF + 4 + 4 * q4;
         float4 v[3];
 #pragma unroll
-        for (int q = 0; q < 3; q++) v[q] = *reinterpret_cast<const float4 *>(cw + q * PF + wy * W + wc);
-        const bool full = xg + 3 < nx;
-        // the row itself and its ghost rows along a periodic y
-        int yrows[3] = {y, 0, 0}, nyr = 1;
-        if (c.pery) {
-          if (y < 2) yrows[nyr++] = y + ny;
-          if (y >= ny - 2) yrows[nyr++] = y - ny;
-        }
-        for (int iy = 0; iy < nyr; iy++) {
-          float *dst = a.out + pbase + (long long)(yrows[iy] + GY) * R.px + (xg + GX);
+        for (int q = 0; q < 3; q++) v[q] = *reinterpret_cast<const float4 *>(cw + q * PF + cell);
+        const bool full = xfirst + 6 < nx;
+        // the row itself, then its ghost copies along a periodic y (y + ny for y < 2, y - ny for y >= ny - 2)
+        const bool g1 = c.pery && y < 2, g2 = c.pery && y >= ny - 2;
+#pragma unroll
+        for (int iy = 0; iy < 3; iy++) {
+          if ((iy == 1 && !g1) || (iy == 2 && !g2)) continue;
+          const int yy = iy == 0 ? y : (iy == 1 ? y + ny : y - ny);
+          float *rowp = a.out + pbase + (long long)(yy + GY) * R.px + h * R.hp + GH;  // half-row, j = 0
+          float *dst = rowp + jl;
           if (full) {
 #pragma unroll
             for (int q = 0; q < 3; q++) *reinterpret_cast<float4 *>(dst + q * R.comp) = v[q];
           } else {
-            for (int e = 0; e < 4 && xg + e < nx; e++)
 #pragma unroll
-              for (int q = 0; q < 3; q++) dst[q * R.comp + e] = elem(v[q], e);
+            for (int e = 0; e < 4; e++)
+              if (xfirst + 2 * e < nx)
+#pragma unroll
+                for (int q = 0; q < 3; q++) dst[q * R.comp + e] = f4get(v[q], e);
           }
-          if (c.perx) {  // ghost columns: x + nx for x < 2, x - nx for x >= nx - 2
-            float *rowp = a.out + pbase + (long long)(yrows[iy] + GY) * R.px + GX;
-            for (int e = 0; e < 4; e++) {
-              const int x = xg + e;
-              if (x >= nx) break;
-              if (x < 2)
+          if (c.perx) {  // ghost columns: x + nx for x < 2 (half index nx/2), x - nx for x >= nx - 2 (index -1)
+            if (jl == 0)
 #pragma unroll
-                for (int q = 0; q < 3; q++) rowp[q * R.comp + x + nx] = elem(v[q], e);
-              if (x >= nx - 2)
+              for (int q = 0; q < 3; q++) rowp[q * R.comp + (nx >> 1)] = v[q].x;
+            const int el = (nx >> 1) - 1 - jl;  // element holding half index nx/2 - 1 (nx is even when periodic)
+            if (el >= 0 && el < 4)
 #pragma unroll
-                for (int q = 0; q < 3; q++) rowp[q * R.comp + x - nx] = elem(v[q], e);
-            }
+              for (int q = 0; q < 3; q++) rowp[q * R.comp - 1] = el == 0 ? v[q].x : (el == 1 ? v[q].y : (el == 2 ? v[q].z : v[q].w));
           }
         }
         if (measure) {
           float f[kPartials];
 #pragma unroll
           for (int q = 0; q < kPartials; q++) f[q] = 0.f;
+          const bool colourA = ((h + y + kw) & 1) == 0;
+          const bool single = colourA && (sid >= 0 || m.field_on);
 #pragma unroll
           for (int e = 0; e < 4; e++) {
-            if (xg + e >= nx) continue;
-            const float vx = elem(v[0], e), vy = elem(v[1], e), vz = elem(v[2], e);
+            if (xfirst + 2 * e >= nx) continue;
+            const float vx = f4get(v[0], e), vy = f4get(v[1], e), vz = f4get(v[2], e);
             f[1] = fmaf(1.5f * vx, vx, f[1] - 0.5f);
             f[2] = fmaf(1.5f * vx, vy, f[2]);
             f[3] = fmaf(1.5f * vx, vz, f[3]);
@@ -477,8 +464,7 @@ __global__ void __launch_bounds__(NT, NT <= 256 ? 2 : 1) k_sweep_fused(ModelDev 
             f[7] += vx;
             f[8] += vy;
             f[9] += vz;
-            if (((xg + e + y + kw) & 1) == 0 && (sid >= 0 || m.field_on))  // colour A: single-site terms
-              f[0] += single_energy(m, Vec3{vx, vy, vz}, sid, Vec3{0.f, 0.f, sz}, c.elecE);
+            if (single) f[0] += single_energy(m, Vec3{vx, vy, vz}, sid, Vec3{0.f, 0.f, sz}, c.elecE);
           }
 #pragma unroll
           for (int q = 0; q < kPartials; q++) dacc[q] += (double)f[q];
@@ -499,6 +485,7 @@ __global__ void __launch_bounds__(NT, NT <= 256 ? 2 : 1) k_sweep_fused(ModelDev 
     __syncthreads();
     return;
   }
+  (void)H;
 
   const unsigned wsum = __reduce_add_sync(0xffffffffu, accepted);
   if ((tid & 31) == 0 && wsum) atomicAdd(&a.st[it.rep].acc, (unsigned long long)wsum);
@@ -543,12 +530,13 @@ bool fused_supported(const mcl_engine *e) {
   return get_encode() != nullptr;
 }
 
-static int encode_map(CUtensorMap *map, float *base, const RepDesc &D, int tx, int ty) {
-  cuuint64_t dims[4] = {(cuuint64_t)D.px, (cuuint64_t)D.py, (cuuint64_t)D.nz, 3};
-  cuuint64_t strides[3] = {(cuuint64_t)D.px * 4, (cuuint64_t)D.px * D.py * 4, (cuuint64_t)D.comp * 4};
-  cuuint32_t box[4] = {(cuuint32_t)(tx + 8), (cuuint32_t)(ty + 4), 1, 3};  // one plane window, 16-byte rows
-  cuuint32_t es[4] = {1, 1, 1, 1};
-  CUresult r = get_encode()(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base + D.off, dims, strides, box, es,
+static int encode_map(CUtensorMap *map, float *base, const RepDesc &D, int ty) {
+  // 5-D view of the split layout: (half-row cell, x parity, padded row, plane, component)
+  cuuint64_t dims[5] = {(cuuint64_t)D.hp, 2, (cuuint64_t)D.py, (cuuint64_t)D.nz, 3};
+  cuuint64_t strides[4] = {(cuuint64_t)D.hp * 4, (cuuint64_t)D.px * 4, (cuuint64_t)D.px * D.py * 4, (cuuint64_t)D.comp * 4};
+  cuuint32_t box[5] = {(cuuint32_t)HALF, 2, (cuuint32_t)(ty + 4), 1, 3};
+  cuuint32_t es[5] = {1, 1, 1, 1, 1};
+  CUresult r = get_encode()(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, base + D.off, dims, strides, box, es,
                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(MCL_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
@@ -606,7 +594,7 @@ static int build_items(mcl_engine *e, FusedPlan *P) {
   std::vector<CUtensorMap> maps(2 * e->n_rep);
   for (int r = 0; r < e->n_rep; r++)
     for (int b = 0; b < 2; b++) {
-      int rc = encode_map(&maps[2 * r + b], e->d_dir[b], e->desc[r], P->tx, P->ty);
+      int rc = encode_map(&maps[2 * r + b], e->d_dir[b], e->desc[r], P->ty);
       if (rc) return rc;
     }
   cudaFree(P->d_tmaps);
@@ -631,7 +619,7 @@ static int build_items(mcl_engine *e, FusedPlan *P) {
   CKF(cudaMalloc(&P->d_first, first.size() * sizeof(int)));
   CKF(cudaMemcpy(P->d_first, first.data(), first.size() * sizeof(int), cudaMemcpyHostToDevice));
   CKF(cudaMalloc(&P->d_partials, (size_t)P->n_items * kPartials * sizeof(double)));
-  const size_t slot_floats = ((size_t)3 * (P->tx + 8) * (P->ty + 4) + 31) / 32 * 32;
+  const size_t slot_floats = ((size_t)3 * RW * (P->ty + 4) + 31) / 32 * 32;
   P->smem = 128 + (size_t)NSL * slot_floats * sizeof(float) + NSL * sizeof(unsigned long long);
   return MCL_OK;
 }
@@ -688,7 +676,7 @@ static cudaError_t launch_one(const mcl_engine *e, const FusedArgs &a) {
 template <int POT, int GEO, bool FLIP>
 static cudaError_t launch_cfg(const mcl_engine *e, const FusedArgs &a) {
   switch (e->fused->cfg) {
-    case 1: return launch_one<POT, GEO, FLIP, 30, 512>(e, a);
+    case 1: return launch_one<POT, GEO, FLIP, 28, 512>(e, a);
     default: return launch_one<POT, GEO, FLIP, 14, 256>(e, a);
   }
 }

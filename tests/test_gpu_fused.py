@@ -71,7 +71,7 @@ def test_fused_equals_untiled(model, shape):
     assert diff.max() <= 2e-6, "max director difference %g" % diff.max()
     assert ava == avb
     np.testing.assert_allclose(sa[0]["energy"], sb[0]["energy"], rtol=2e-6, atol=2e-6)
-    np.testing.assert_allclose(sa[0]["q"], sb[0]["q"], rtol=0, atol=1e-6)
+    np.testing.assert_allclose(sa[0]["q"], sb[0]["q"], rtol=0, atol=2e-7)
     np.testing.assert_array_equal(sa[0]["acceptance"], sb[0]["acceptance"])
 
 
