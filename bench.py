@@ -37,29 +37,74 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-NX = NY = NZ = 256
-T = 0.8
-SEED = 7
 BYTES_PER_SITE_UPDATE = 24
 METRIC = "site-updates/s"
-WORKLOAD = "ghrl_slab_256^3_k1:0.5:1.5_homeotropic_W1.5_T0.8"
+SEED = 7
+
+
+def c3_sizes(seed=11, n=64):
+    """C3's replica sizes: L = 2 round(exp(U(ln 16, ln 128)) / 2) from a seeded numpy stream."""
+    rng = np.random.default_rng(seed)
+    return [int(2 * round(np.exp(rng.uniform(np.log(16), np.log(128))) / 2)) for _ in range(n)]
+
+
+def workload(name):
+    """Model, replicas and descriptive config of a named workload (synthetic lattices of the configs' shapes)."""
+    import mclics_b200 as M
+    if name == "c2":
+        model = M.Model("ghrl", k=(1.0, 0.5, 1.5), surfaces=[("homeotropic", 1.5, 0, 0)] * 2)
+        reps = [dict(nx=256, ny=256, nz=256, geometry="slab", periodic=(1, 1, 0), T=0.8, seed=7)]
+        cfg = {"workload": "ghrl_slab_256^3_k1:0.5:1.5_homeotropic_W1.5_T0.8", "geometry": "slab",
+               "potential": "ghrl", "lattices": "1 x 256^3", "k11_k22_k33": [1, 0.5, 1.5],
+               "anchoring": "homeotropic W=1.5 (both plates)", "T": 0.8}
+        ic = "z_noise"
+    elif name == "c1":
+        model = M.Model("ll")
+        reps = [dict(nx=32, ny=32, nz=32, geometry="bulk", periodic=(1, 1, 1), T=1.1, seed=1)]
+        cfg = {"workload": "ll_bulk_32^3_T1.1", "potential": "ll", "lattices": "1 x 32^3", "T": 1.1}
+        ic = "random"
+    elif name == "c3":
+        sizes = c3_sizes()
+        model = M.Model("ll")
+        reps = [dict(nx=L, ny=L, nz=L, geometry="bulk", periodic=(1, 1, 1), T=1.0 + 0.2 * r / 63, seed=r + 1)
+                for r, L in enumerate(sizes)]
+        cfg = {"workload": "ll_64_replicas_16^3-128^3_T1.00-1.20", "potential": "ll",
+               "lattices": "64 replicas, L from 2 round(exp(U(ln16, ln128))/2), seed 11",
+               "sites": int(sum(L ** 3 for L in sizes))}
+        ic = "random"
+    elif name == "c4":
+        model = M.Model("ll")
+        reps = [dict(nx=128, ny=128, nz=128, geometry="bulk", periodic=(1, 1, 1), T=T, seed=3 + i)
+                for i, T in enumerate((0.3, 0.8, 1.12))]
+        cfg = {"workload": "ll_bulk_128^3_T0.3_0.8_1.12", "potential": "ll", "lattices": "3 x 128^3 (one per T)"}
+        ic = "random"
+    elif name == "c5":
+        model = M.Model("pear", field_dir=(0, 0, 1), elecP=1.0, surfaces=[("fg", 1.0, 0, 0)] * 2)
+        reps = [dict(nx=256, ny=256, nz=64, geometry="slab", periodic=(1, 1, 0), T=0.5, elecE=2.0 * i / 31, seed=5 + i)
+                for i in range(32)]
+        cfg = {"workload": "pear_slab_256x256x64_32_fields_0-2_T0.5", "potential": "pear", "geometry": "slab",
+               "lattices": "32 replicas (field 0..2 along z, elecP=1, fg W=1)", "T": 0.5}
+        ic = "random"
+    else:
+        raise SystemExit("unknown workload " + name)
+    return model, reps, cfg, ic
+
+
+def initial_state(n, kind, seed):
+    rng = np.random.default_rng(seed)
+    if kind == "z_noise":  # (0, 0, 1) + uniform noise of amplitude 0.1 per component, renormalised
+        v = rng.uniform(-0.1, 0.1, size=(n, 3)).astype(np.float32)
+        v[:, 2] += 1.0
+    else:
+        v = rng.normal(size=(n, 3)).astype(np.float32)
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    return v.reshape(-1).astype(np.float32)
 
 
 def c2_input_text():
-    return ("Nx %d\nNy %d\nNz %d\ngeometry slab\nxbound periodic\nybound periodic\npotential ghrl\nk11 1\nk22 0.5\n"
+    return ("Nx 256\nNy 256\nNz 256\ngeometry slab\nxbound periodic\nybound periodic\npotential ghrl\nk11 1\nk22 0.5\n"
             "k33 1.5\nanchoring_type 0 homeotropic\nW 0 1.5\nanchoring_type 1 homeotropic\nW 1 1.5\nevol thermal\n"
-            "Ti %g\nTf %g\ndT -0.1\nMCT 200\nMCS 1000\nic homogeneous\ntheta_0 0\nphi_0 0\nseed %d\n"
-            % (NX, NY, NZ, T, T, SEED))
-
-
-def c2_initial_state(seed=SEED):
-    """(0, 0, 1) + uniform noise of amplitude 0.1 per component, renormalised (seeded numpy stream)."""
-    rng = np.random.default_rng(seed)
-    n = NX * NY * NZ
-    v = rng.uniform(-0.1, 0.1, size=(n, 3)).astype(np.float32)
-    v[:, 2] += 1.0
-    v /= np.linalg.norm(v, axis=1, keepdims=True)
-    return v.reshape(-1).astype(np.float32)
+            "Ti 0.8\nTf 0.8\ndT -0.1\nMCT 200\nMCS 1000\nic homogeneous\ntheta_0 0\nphi_0 0\nseed 7\n")
 
 
 def measured_peaks():
@@ -130,7 +175,8 @@ class ClockSampler:
 
 
 def reference_cpu(steps, warmup, budget_s=150.0):
-    """Times the reference's own CPU sweep + measurement (oracle/_ref/mclics_ref_timing) on all host cores."""
+    """Times the reference's own CPU sweep + measurement (oracle/_ref/mclics_ref_timing) on all host cores, on the
+    256^3 GHRL slab."""
     exe = os.path.join(ROOT, "oracle", "_ref", "mclics_ref_timing")
     if not os.path.exists(exe):
         return None, "oracle/_ref/mclics_ref_timing not built"
@@ -164,14 +210,15 @@ def gpu_arm(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    model = M.Model("ghrl", k=(1.0, 0.5, 1.5), surfaces=[("homeotropic", 1.5, 0, 0)] * 2)
-    rep = M.Replica(NX, NY, NZ, "slab", (1, 1, 0), T=T, seed=SEED + 1000 * rank)
-    eng = M.Engine(model, [rep])
-    ni0 = c2_initial_state(SEED + rank)
-    eng.upload(0, ni0)
+    model, reps, cfg, ic = workload(args.workload)
+    creps = [M.Replica(**dict(r, seed=r["seed"] + 1000 * rank)) for r in reps]
+    eng = M.Engine(model, creps)
+    sizes = [r["nx"] * r["ny"] * r["nz"] for r in reps]
+    for i, n in enumerate(sizes):
+        eng.upload(i, initial_state(n, ic, SEED + 97 * i + rank))
     stream = torch.cuda.Stream(device=dev)
     eng.set_stream(stream.cuda_stream)
-    sites = NX * NY * NZ
+    sites = sum(sizes)
 
     for _ in range(args.warmup):
         eng.sweeps(1, measure=True)
@@ -199,18 +246,20 @@ def gpu_arm(args, rank, world, local_rank):
     launches = l1 - l0
     rec = eng.series(0, eng.series_length() - 1, 1)[0]
 
-    # end to end through the C ABI with host buffers
-    host_ni = torch.empty(3 * sites, dtype=torch.float32, pin_memory=True)
-    host_T = torch.tensor([T], dtype=torch.float32, pin_memory=True)
+    # end to end through the C ABI with host buffers (reference GPU loop data movement, all replicas)
+    host_ni = [torch.empty(3 * n, dtype=torch.float32, pin_memory=True) for n in sizes]
+    host_T = torch.tensor([r["T"] for r in reps], dtype=torch.float32, pin_memory=True)
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        eng.set_temperature(float(host_T[0]))
+        for i in range(len(reps)):
+            eng.set_temperature(float(host_T[i]), i)
         eng.sweeps(1, measure=True)
-        eng.series(0, eng.series_length() - 1, 1)
-        M.check(M.lib().mcl_download_directors(eng._h, 0, host_ni.data_ptr()))
+        for i in range(len(reps)):
+            eng.series(i, eng.series_length() - 1, 1)
+            M.check(M.lib().mcl_download_directors(eng._h, i, host_ni[i].data_ptr()))
     e2e_s = time.perf_counter() - t0
 
     times = torch.tensor([dev_ms, e2e_s * 1e3], dtype=torch.float64, device=dev)
@@ -219,7 +268,8 @@ def gpu_arm(args, rank, world, local_rank):
     dev_ms_max, e2e_ms_max = float(times[0]), float(times[1])
     eng.close()
     return dict(dev_ms=dev_ms_max, e2e_ms=e2e_ms_max, kernel_ms=kernel_ms, launches=launches, sites=sites,
-                clocks=clocks.summary(), S=float(rec["S"]), E=float(rec["energy"]), acc=float(rec["acceptance"]))
+                n_rep=len(reps), clocks=clocks.summary(), S=float(rec["S"]), E=float(rec["energy"]),
+                acc=float(rec["acceptance"]), cfg=cfg)
 
 
 def main():
@@ -229,17 +279,17 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="mclics_b200", choices=["mclics_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"],
+                    help="c2 (default): the headline GHRL 256^3 slab; others: the remaining configurations")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-    config = {"workload": WORKLOAD, "lattice": [NX, NY, NZ], "geometry": "slab", "potential": "ghrl",
-              "k11_k22_k33": [1, 0.5, 1.5], "anchoring": "homeotropic W=1.5 (both plates)", "T": T,
-              "step": "1 sweep + measurement", "global_sites_per_step": NX * NY * NZ * max(1, args.gpus),
-              "parallelism": "independent replicas x%d" % max(1, args.gpus),
-              "l2": "inputs larger than L2 (211 MB padded lattice > 126 MB)"}
+    _, _, config, _ = workload(args.workload) if args.impl != "reference" else workload("c2")
+    config = dict(config, step="1 sweep + measurement of every lattice",
+                  parallelism="independent replicas x%d" % max(1, args.gpus))
 
     if args.impl == "reference":
         if rank != 0:
@@ -266,7 +316,7 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     res = gpu_arm(args, rank, world, local_rank)
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "c2":
         r, why = reference_cpu(10, 1, budget_s=25.0)
         if r is not None:
             cpu = {"value": r["sites"] * r["steps"] / r["seconds"], "unit": "site-updates/s", "cores": r["threads"],
@@ -282,6 +332,10 @@ def main():
     if rank != 0:
         return 0
     sites_total = res["sites"] * world
+    config["global_sites_per_step"] = sites_total
+    config["l2"] = ("inputs larger than L2 (%.0f MB of directors > 126 MB)" % (res["sites"] * 12 / 1e6)
+                    if res["sites"] * 12 > 126e6 else
+                    "inputs smaller than L2 (%.0f MB): DRAM roofline is an upper bound" % (res["sites"] * 12 / 1e6))
     value = sites_total * args.steps / (res["dev_ms"] / 1e3)
     e2e = sites_total * args.steps / (res["e2e_ms"] / 1e3)
     peak, peak_kind = measured_peaks()
@@ -291,15 +345,15 @@ def main():
         "warmup": args.warmup, "ms_per_step": res["dev_ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 (f64 accumulators)", "data": "synthetic", "config": config,
         "e2e": {"value": e2e, "unit": "site-updates/s", "h2d_bytes_per_step": 4,
-                "d2h_bytes_per_step": 144 + 12 * res["sites"]},
+                "d2h_bytes_per_step": 144 * res["n_rep"] + 12 * res["sites"]},
         "gpu_launches": res["launches"],
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": peak_kind, "traffic": ncu_traffic("sweep_ghrl_slab_256"),
+                     "peak_kind": peak_kind, "traffic": ncu_traffic(args.workload),
                      "kernel_ms_per_sweep": res["kernel_ms"],
                      "algorithmic_bytes_per_sweep": res["sites"] * BYTES_PER_SITE_UPDATE},
         "cpu_baseline": cpu,
         "clocks": res["clocks"],
-        "physics": {"S_last": res["S"], "E_last": res["E"], "acceptance_last": res["acc"]},
+        "physics": {"S_last_replica0": res["S"], "E_last_replica0": res["E"], "acceptance_last_replica0": res["acc"]},
     }
     print(json.dumps(line))
     return 0

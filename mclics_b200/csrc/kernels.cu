@@ -41,15 +41,17 @@ __global__ void __launch_bounds__(kThreads) k_sweep_color(ModelDev m, const RepD
       const float T = S.T, invT = 1.f / T;
       const long long site = site_linear(R, x, y, z);
       const Draw d = site_draw(R.seed, *sweep_ctr, x, y, z, R.nx, R.ny, m.flip);
-      const SiteResult r = m.flip ? site_update<POT, true>(m, n, nb, w, sid, s, S.elecE, d, S.ang_var, T, invT)
-                                  : site_update<POT, false>(m, n, nb, w, sid, s, S.elecE, d, S.ang_var, T, invT);
-      accepted = r.rot;
-      if (r.rot | r.flip) {
+      const LaneDraw<float> ld = lane_draw(d, m.flip);
+      const SiteResultT<float> r =
+          m.flip ? site_update<POT, true, float>(m, n, nb, w, sid, s, S.elecE, ld, S.ang_var, T, invT)
+                 : site_update<POT, false, float>(m, n, nb, w, sid, s, S.elecE, ld, S.ang_var, T, invT);
+      accepted = r.rot ? 1u : 0u;
+      if (r.rot || r.flip) {
         dir[dir_index(R, 0, x, y, z)] = r.n.x;
         dir[dir_index(R, 1, x, y, z)] = r.n.y;
         dir[dir_index(R, 2, x, y, z)] = r.n.z;
       }
-      if (dec) dec[R.site_off + site] = (uint8_t)(0x80u | r.rot | (r.flip << 1));
+      if (dec) dec[R.site_off + site] = (uint8_t)(0x80u | (r.rot ? 1u : 0u) | (r.flip ? 2u : 0u));
     }
   }
   const unsigned wsum = __reduce_add_sync(0xffffffffu, accepted);

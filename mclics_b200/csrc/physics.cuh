@@ -1,5 +1,9 @@
-// Site energies and the trial move for the production kernels: FP32, explicit fmaf everywhere it matters, so
-// that every kernel that calls these functions (untiled and fused) rounds identically.
+// Site energies and the trial move for the production kernels, written once over a lane type L:
+//   L = float   one site per thread (untiled kernels),
+//   L = float2  two sites per thread, computed with Blackwell's paired FP32 instructions (FFMA2/FMUL2/FADD2:
+//               __ffma2_rn, __fmul2_rn, __fadd2_rn), one site per lane.
+// Every floating-point operation is explicit (fmaf / __fmul_rn / __fadd_rn or their paired forms), so both lane
+// types round identically and the fused and untiled kernels take the same decisions.
 //
 // Definitions follow the reference CPU code (src/potential.cpp:19-63, src/anchoring_*.cpp,
 // src/geometry*.cpp site_energy): E_site = sum over present neighbours of U(n, n_j, r_j) + [surface] anchoring
@@ -10,11 +14,60 @@
 
 namespace mcl {
 
-struct Vec3 {
-  float x, y, z;
+// ---- lane operations ---------------------------------------------------------------------------------------
+struct B2 {
+  bool x, y;
 };
-__device__ __forceinline__ float dot(const Vec3 &a, const Vec3 &b) { return fmaf(a.x, b.x, fmaf(a.y, b.y, a.z * b.z)); }
-__device__ __forceinline__ float comp(const Vec3 &a, int c) { return c == 0 ? a.x : (c == 1 ? a.y : a.z); }
+template <typename L>
+struct LaneBool;
+template <>
+struct LaneBool<float> {
+  using type = bool;
+};
+template <>
+struct LaneBool<float2> {
+  using type = B2;
+};
+template <typename L>
+using LB = typename LaneBool<L>::type;
+
+__device__ __forceinline__ float fma_(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ float2 fma_(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float mul_(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float2 mul_(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float add_(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float2 add_(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float neg_(float a) { return -a; }
+__device__ __forceinline__ float2 neg_(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ float sub_(float a, float b) { return __fadd_rn(a, -b); }
+__device__ __forceinline__ float2 sub_(float2 a, float2 b) { return __fadd2_rn(a, neg_(b)); }
+template <typename L>
+__device__ __forceinline__ L splat(float v);
+template <>
+__device__ __forceinline__ float splat<float>(float v) { return v; }
+template <>
+__device__ __forceinline__ float2 splat<float2>(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float sel_(bool c, float a, float b) { return c ? a : b; }
+__device__ __forceinline__ float2 sel_(B2 c, float2 a, float2 b) { return make_float2(c.x ? a.x : b.x, c.y ? a.y : b.y); }
+__device__ __forceinline__ bool gt0(float a) { return a > 0.f; }
+__device__ __forceinline__ B2 gt0(float2 a) { return B2{a.x > 0.f, a.y > 0.f}; }
+__device__ __forceinline__ float sign_(float b) { return b > 0.f ? 1.f : -1.f; }
+__device__ __forceinline__ float2 sign_(float2 b) { return make_float2(b.x > 0.f ? 1.f : -1.f, b.y > 0.f ? 1.f : -1.f); }
+
+template <typename L>
+struct V3 {
+  L x, y, z;
+};
+using Vec3 = V3<float>;
+
+template <typename L>
+__device__ __forceinline__ L dot(const V3<L> &a, const V3<L> &b) {
+  return fma_(a.x, b.x, fma_(a.y, b.y, mul_(a.z, b.z)));
+}
+template <int C, typename L>
+__device__ __forceinline__ L comp(const V3<L> &a) {
+  return C == 0 ? a.x : (C == 1 ? a.y : a.z);
+}
 
 // Bond D = 0..5 is +x, -x, +y, -y, +z, -z: axis D/2, sign +1 for even D.
 template <int D>
@@ -24,29 +77,31 @@ struct BondDir {
 };
 
 // Lebwohl-Lasher, src/potential.cpp:28-31: -1.5 A (n.n_j)^2.
-__device__ __forceinline__ float ll_bond(const ModelDev &m, const Vec3 &x, const Vec3 &y) {
-  const float b = dot(x, y);
-  return __fmul_rn(-1.5f * m.A, __fmul_rn(b, b));
+template <typename L>
+__device__ __forceinline__ L ll_bond(const ModelDev &m, const V3<L> &x, const V3<L> &y) {
+  const L b = dot(x, y);
+  return mul_(splat<L>(-1.5f * m.A), mul_(b, b));
 }
 
 // GHRL with bond vector r = sign * e_axis, src/potential.cpp:40-56.
-template <int AXIS>
-__device__ __forceinline__ float ghrl_bond(const ModelDev &m, const Vec3 &x, const Vec3 &y, float sign) {
-  const float ai = comp(x, AXIS), aj = comp(y, AXIS);  // a_i a_j and a^2 do not depend on the sign of r
-  const float b = dot(x, y);
-  const float p2 = fmaf(__fmul_rn(1.5f, b), b, -0.5f);
-  const float e1 = fmaf(1.5f, fmaf(ai, ai, __fmul_rn(aj, aj)), -1.f);
-  float u = fmaf(e1, fmaf(m.rho, p2, m.lam), fmaf(m.mu, fmaf(__fmul_rn(ai, aj), b, -1.f / 9.f), __fmul_rn(m.nu, p2)));
+template <int AXIS, typename L>
+__device__ __forceinline__ L ghrl_bond(const ModelDev &m, const V3<L> &x, const V3<L> &y, float sign) {
+  const L ai = comp<AXIS>(x), aj = comp<AXIS>(y);  // a_i a_j and a^2 do not depend on the sign of r
+  const L b = dot(x, y);
+  const L p2 = fma_(mul_(splat<L>(1.5f), b), b, splat<L>(-0.5f));
+  const L e1 = fma_(splat<L>(1.5f), fma_(ai, ai, mul_(aj, aj)), splat<L>(-1.f));
+  L u = fma_(e1, fma_(splat<L>(m.rho), p2, splat<L>(m.lam)),
+             fma_(splat<L>(m.mu), fma_(mul_(ai, aj), b, splat<L>(-1.f / 9.f)), mul_(splat<L>(m.nu), p2)));
   if (m.sigma != 0.f) {
     // c = r . (n_j x n_i)
-    const float c = AXIS == 0 ? fmaf(y.y, x.z, -__fmul_rn(y.z, x.y))
-                              : (AXIS == 1 ? fmaf(y.z, x.x, -__fmul_rn(y.x, x.z)) : fmaf(y.x, x.y, -__fmul_rn(y.y, x.x)));
-    u = fmaf(__fmul_rn(m.sigma * sign, b > 0.f ? 1.f : -1.f), c, u);
+    const L c = AXIS == 0 ? fma_(y.y, x.z, neg_(mul_(y.z, x.y)))
+                          : (AXIS == 1 ? fma_(y.z, x.x, neg_(mul_(y.x, x.z))) : fma_(y.x, x.y, neg_(mul_(y.y, x.x))));
+    u = fma_(mul_(splat<L>(m.sigma * sign), sign_(b)), c, u);
   }
   return u;
 }
 
-// GHRL with an arbitrary bond vector (anchoring phantom neighbour along the surface normal).
+// GHRL with an arbitrary bond vector (anchoring phantom neighbour along the surface normal), one site.
 __device__ __forceinline__ float ghrl_general(const ModelDev &m, const Vec3 &x, const Vec3 &y, const Vec3 &r) {
   const float ai = dot(x, r), aj = dot(y, r), b = dot(x, y);
   const float p2 = fmaf(__fmul_rn(1.5f, b), b, -0.5f);
@@ -61,37 +116,40 @@ __device__ __forceinline__ float ghrl_general(const ModelDev &m, const Vec3 &x, 
 }
 
 // Pear (Dhakal & Selinger), src/potential.cpp:19-24: -A b^2 - B1 b - C/4 (1+b)^2 r.(n_j - n_i).
-template <int AXIS>
-__device__ __forceinline__ float pear_bond(const ModelDev &m, const Vec3 &x, const Vec3 &y, float sign) {
-  const float b = dot(x, y);
-  const float opb = 1.f + b;
-  const float ps = __fmul_rn(__fmul_rn(opb, opb), sign * (comp(y, AXIS) - comp(x, AXIS)));
-  return fmaf(__fmul_rn(-m.A, b), b, fmaf(-m.B1, b, __fmul_rn(-0.25f * m.C, ps)));
+template <int AXIS, typename L>
+__device__ __forceinline__ L pear_bond(const ModelDev &m, const V3<L> &x, const V3<L> &y, float sign) {
+  const L b = dot(x, y);
+  const L opb = add_(splat<L>(1.f), b);
+  const L diff = sub_(comp<AXIS>(y), comp<AXIS>(x));
+  const L ps = mul_(mul_(opb, opb), sign > 0.f ? diff : neg_(diff));
+  return fma_(mul_(splat<L>(-m.A), b), b, fma_(splat<L>(-m.B1), b, mul_(splat<L>(-0.25f * m.C), ps)));
 }
 
-template <int POT, int D>
-__device__ __forceinline__ float bond(const ModelDev &m, const Vec3 &x, const Vec3 &y) {
+template <int POT, int D, typename L>
+__device__ __forceinline__ L bond(const ModelDev &m, const V3<L> &x, const V3<L> &y) {
   if (POT == POT_LL) return ll_bond(m, x, y);
   if (POT == POT_GHRL) return ghrl_bond<BondDir<D>::axis>(m, x, y, BondDir<D>::sign);
   return pear_bond<BondDir<D>::axis>(m, x, y, BondDir<D>::sign);
 }
 
 // Sum over the six bonds with weights w[d] in {0, 1} (0: free edge or empty site).
-template <int POT>
-__device__ __forceinline__ float bond_sum(const ModelDev &m, const Vec3 &x, const Vec3 (&nb)[6], const float (&w)[6]) {
-  float e = __fmul_rn(w[0], bond<POT, 0>(m, x, nb[0]));
-  e = fmaf(w[1], bond<POT, 1>(m, x, nb[1]), e);
-  e = fmaf(w[2], bond<POT, 2>(m, x, nb[2]), e);
-  e = fmaf(w[3], bond<POT, 3>(m, x, nb[3]), e);
-  e = fmaf(w[4], bond<POT, 4>(m, x, nb[4]), e);
-  e = fmaf(w[5], bond<POT, 5>(m, x, nb[5]), e);
+template <int POT, typename L>
+__device__ __forceinline__ L bond_sum(const ModelDev &m, const V3<L> &x, const V3<L> (&nb)[6], const L (&w)[6]) {
+  L e = mul_(w[0], bond<POT, 0>(m, x, nb[0]));
+  e = fma_(w[1], bond<POT, 1>(m, x, nb[1]), e);
+  e = fma_(w[2], bond<POT, 2>(m, x, nb[2]), e);
+  e = fma_(w[3], bond<POT, 3>(m, x, nb[3]), e);
+  e = fma_(w[4], bond<POT, 4>(m, x, nb[4]), e);
+  e = fma_(w[5], bond<POT, 5>(m, x, nb[5]), e);
   return e;
 }
 
 // Field, src/potential.cpp:59-63.
-__device__ __forceinline__ float field_energy(const ModelDev &m, const Vec3 &x, float elecE) {
-  const float ne = __fmul_rn(elecE, fmaf(x.x, m.fdir[0], fmaf(x.y, m.fdir[1], __fmul_rn(x.z, m.fdir[2]))));
-  return fmaf(-m.elecA, __fmul_rn(ne, ne), __fmul_rn(-m.elecP, ne));
+template <typename L>
+__device__ __forceinline__ L field_energy(const ModelDev &m, const V3<L> &x, float elecE) {
+  const L ne = mul_(splat<L>(elecE),
+                    fma_(x.x, splat<L>(m.fdir[0]), fma_(x.y, splat<L>(m.fdir[1]), mul_(x.z, splat<L>(m.fdir[2])))));
+  return fma_(splat<L>(-m.elecA), mul_(ne, ne), mul_(splat<L>(-m.elecP), ne));
 }
 
 // Anchoring of surface sid for a site with outward normal s (src/anchoring_*.cpp surface_potential, W included).
@@ -136,71 +194,120 @@ __device__ __forceinline__ float anchoring_energy(const ModelDev &m, int sid, co
   return 0.f;
 }
 
-// Single-site terms: anchoring (sid >= 0) and field.
+// Single-site terms: anchoring (sid >= 0, the same surface for both lanes) and field.
 __device__ __forceinline__ float single_energy(const ModelDev &m, const Vec3 &x, int sid, const Vec3 &s, float elecE) {
   float e = 0.f;
   if (sid >= 0) e = anchoring_energy(m, sid, x, s);
   if (m.field_on) e = __fadd_rn(e, field_energy(m, x, elecE));
   return e;
 }
+__device__ __forceinline__ float2 single_energy(const ModelDev &m, const V3<float2> &x, int sid, const Vec3 &s,
+                                                float elecE) {
+  float2 e = make_float2(0.f, 0.f);
+  if (sid >= 0) {
+    e.x = anchoring_energy(m, sid, Vec3{x.x.x, x.y.x, x.z.x}, s);
+    e.y = anchoring_energy(m, sid, Vec3{x.x.y, x.y.y, x.z.y}, s);
+  }
+  if (m.field_on) e = __fadd2_rn(e, field_energy(m, x, elecE));
+  return e;
+}
+
+// Per-lane transcendental helpers.
+__device__ __forceinline__ void sincos_pi(float va, float &s, float &c) { __sincosf(__fmul_rn(3.14159265358979f, va), &s, &c); }
+__device__ __forceinline__ void sincos_pi(float2 va, float2 &s, float2 &c) {
+  sincos_pi(va.x, s.x, c.x);
+  sincos_pi(va.y, s.y, c.y);
+}
+__device__ __forceinline__ float rsqrt_(float a) { return rsqrtf(a); }
+__device__ __forceinline__ float2 rsqrt_(float2 a) { return make_float2(rsqrtf(a.x), rsqrtf(a.y)); }
 
 // Trial rotation by pi * va about axis `axis` (src/evolve.cpp:153-176): the reference's three rotations in one
-// branch-free Rodrigues form n' = c n + (1 - c) n_a e_a - s (e_a x n), then renormalised.
-__device__ __forceinline__ Vec3 rotate_trial(const Vec3 &n, float va, int axis) {
-  float s, c;
-  __sincosf(__fmul_rn(3.14159265358979f, va), &s, &c);  // |pi va| <= pi: the hardware sin/cos range
-  const float w0 = axis == 0 ? 1.f : 0.f, w1 = axis == 1 ? 1.f : 0.f, w2 = axis == 2 ? 1.f : 0.f;
-  const float cx = fmaf(w1, n.z, -__fmul_rn(w2, n.y)), cy = fmaf(w2, n.x, -__fmul_rn(w0, n.z)),
-              cz = fmaf(w0, n.y, -__fmul_rn(w1, n.x));
-  const float omc = 1.f - c;
-  const Vec3 r{fmaf(c, n.x, fmaf(__fmul_rn(omc, w0), n.x, -__fmul_rn(s, cx))),
-               fmaf(c, n.y, fmaf(__fmul_rn(omc, w1), n.y, -__fmul_rn(s, cy))),
-               fmaf(c, n.z, fmaf(__fmul_rn(omc, w2), n.z, -__fmul_rn(s, cz)))};
-  const float inv = rsqrtf(dot(r, r));
-  return Vec3{__fmul_rn(r.x, inv), __fmul_rn(r.y, inv), __fmul_rn(r.z, inv)};
+// branch-free Rodrigues form n' = c n + (1 - c) n_a e_a - s (e_a x n), then renormalised. w0..w2: one-hot axis.
+template <typename L>
+__device__ __forceinline__ V3<L> rotate_trial(const V3<L> &n, L va, L w0, L w1, L w2) {
+  L s, c;
+  sincos_pi(va, s, c);  // |pi va| <= pi: the hardware sin/cos range
+  const L cx = fma_(w1, n.z, neg_(mul_(w2, n.y))), cy = fma_(w2, n.x, neg_(mul_(w0, n.z))),
+          cz = fma_(w0, n.y, neg_(mul_(w1, n.x)));
+  const L omc = sub_(splat<L>(1.f), c);
+  const V3<L> r{fma_(c, n.x, fma_(mul_(omc, w0), n.x, neg_(mul_(s, cx)))),
+                fma_(c, n.y, fma_(mul_(omc, w1), n.y, neg_(mul_(s, cy)))),
+                fma_(c, n.z, fma_(mul_(omc, w2), n.z, neg_(mul_(s, cz))))};
+  const L inv = rsqrt_(dot(r, r));
+  return V3<L>{mul_(r.x, inv), mul_(r.y, inv), mul_(r.z, inv)};
 }
 
 // Metropolis test u < exp(-dE/T); T = 0 accepts when the energy does not increase (src/evolve.cpp:185-188).
 __device__ __forceinline__ bool metropolis(float u, float dE, float invT, float T) {
   return T > 0.f ? (u < __expf(-__fmul_rn(dE, invT))) : (dE <= 0.f);
 }
+__device__ __forceinline__ B2 metropolis(float2 u, float2 dE, float invT, float T) {
+  return B2{metropolis(u.x, dE.x, invT, T), metropolis(u.y, dE.y, invT, T)};
+}
 
-// Result of one trial move of one site.
-struct SiteResult {
-  Vec3 n;          // director after the move
-  float bond;      // bond energy of the final director
-  float single;    // single-site energy of the final director
-  unsigned rot;    // 1 if the rotation was accepted
-  unsigned flip;   // 1 if the flip was accepted
+// Draw fields -> lane values.
+template <typename L>
+struct LaneDraw {
+  L u1, u3, u4;   // angle, rotation acceptance, flip acceptance uniforms
+  L w0, w1, w2;   // one-hot rotation axis
+};
+__device__ __forceinline__ LaneDraw<float> lane_draw(const Draw &d, bool flip) {
+  LaneDraw<float> r;
+  r.u1 = unif(d.f1, flip);
+  r.u3 = unif(d.f3, flip);
+  r.u4 = unif(d.f4, flip);
+  const int a = rotation_axis(d.f2, flip);
+  r.w0 = a == 0 ? 1.f : 0.f;
+  r.w1 = a == 1 ? 1.f : 0.f;
+  r.w2 = a == 2 ? 1.f : 0.f;
+  return r;
+}
+__device__ __forceinline__ LaneDraw<float2> lane_draw(const Draw &d0, const Draw &d1, bool flip) {
+  const LaneDraw<float> a = lane_draw(d0, flip), b = lane_draw(d1, flip);
+  return LaneDraw<float2>{make_float2(a.u1, b.u1), make_float2(a.u3, b.u3), make_float2(a.u4, b.u4),
+                          make_float2(a.w0, b.w0), make_float2(a.w1, b.w1), make_float2(a.w2, b.w2)};
+}
+
+// Result of one trial move per lane.
+template <typename L>
+struct SiteResultT {
+  V3<L> n;       // director after the move
+  L bond;        // bond energy of the final director
+  L single;      // single-site energy of the final director
+  LB<L> rot;     // rotation accepted
+  LB<L> flip;    // flip accepted
 };
 
+template <typename L>
+__device__ __forceinline__ V3<L> sel3(LB<L> c, const V3<L> &a, const V3<L> &b) {
+  return V3<L>{sel_(c, a.x, b.x), sel_(c, a.y, b.y), sel_(c, a.z, b.z)};
+}
+
 // One trial move (src/evolve.cpp:133-207): rotation, Metropolis, then the optional n -> -n trial.
-template <int POT, bool FLIP>
-__device__ __forceinline__ SiteResult site_update(const ModelDev &m, const Vec3 &n, const Vec3 (&nb)[6],
-                                                  const float (&w)[6], int sid, const Vec3 &s, float elecE,
-                                                  const Draw &d, float av, float T, float invT) {
-  const float va = __fmul_rn(fmaf(2.f, unif(d.f1, FLIP), -1.f), av);
-  const Vec3 nn = rotate_trial(n, va, rotation_axis(d.f2, FLIP));
-  const float b_old = bond_sum<POT>(m, n, nb, w), b_new = bond_sum<POT>(m, nn, nb, w);
-  const float s_old = single_energy(m, n, sid, s, elecE), s_new = single_energy(m, nn, sid, s, elecE);
-  const float e_old = __fadd_rn(b_old, s_old), e_new = __fadd_rn(b_new, s_new);
-  SiteResult r;
-  const bool acc = metropolis(unif(d.f3, FLIP), __fsub_rn(e_new, e_old), invT, T);
-  r.n = acc ? nn : n;
-  r.bond = acc ? b_new : b_old;
-  r.single = acc ? s_new : s_old;
-  r.rot = acc ? 1u : 0u;
-  r.flip = 0u;
+template <int POT, bool FLIP, typename L>
+__device__ __forceinline__ SiteResultT<L> site_update(const ModelDev &m, const V3<L> &n, const V3<L> (&nb)[6],
+                                                      const L (&w)[6], int sid, const Vec3 &s, float elecE,
+                                                      const LaneDraw<L> &d, float av, float T, float invT) {
+  const L va = mul_(fma_(splat<L>(2.f), d.u1, splat<L>(-1.f)), splat<L>(av));
+  const V3<L> nn = rotate_trial(n, va, d.w0, d.w1, d.w2);
+  const L b_old = bond_sum<POT>(m, n, nb, w), b_new = bond_sum<POT>(m, nn, nb, w);
+  const L s_old = single_energy(m, n, sid, s, elecE), s_new = single_energy(m, nn, sid, s, elecE);
+  const L e_old = add_(b_old, s_old), e_new = add_(b_new, s_new);
+  SiteResultT<L> r;
+  r.rot = metropolis(d.u3, sub_(e_new, e_old), invT, T);
+  r.n = sel3<L>(r.rot, nn, n);
+  r.bond = sel_(r.rot, b_new, b_old);
+  r.single = sel_(r.rot, s_new, s_old);
   if (FLIP) {
-    const Vec3 f{-r.n.x, -r.n.y, -r.n.z};
-    const float bf = bond_sum<POT>(m, f, nb, w), sf = single_energy(m, f, sid, s, elecE);
-    const float e_cur = __fadd_rn(r.bond, r.single);
-    if (metropolis(unif(d.f4, FLIP), __fsub_rn(__fadd_rn(bf, sf), e_cur), invT, T)) {
-      r.n = f;
-      r.bond = bf;
-      r.single = sf;
-      r.flip = 1u;
-    }
+    const V3<L> f{neg_(r.n.x), neg_(r.n.y), neg_(r.n.z)};
+    const L bf = bond_sum<POT>(m, f, nb, w), sf = single_energy(m, f, sid, s, elecE);
+    const L e_cur = add_(r.bond, r.single);
+    r.flip = metropolis(d.u4, sub_(add_(bf, sf), e_cur), invT, T);
+    r.n = sel3<L>(r.flip, f, r.n);
+    r.bond = sel_(r.flip, bf, r.bond);
+    r.single = sel_(r.flip, sf, r.single);
+  } else {
+    r.flip = LB<L>{};
   }
   return r;
 }

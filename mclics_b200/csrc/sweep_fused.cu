@@ -184,48 +184,53 @@ __device__ __forceinline__ void pair_task(const ModelDev &m, const Ctx &c, float
   const int yw = c.pery ? (y < 0 ? y + c.ny : (y >= c.ny ? y - c.ny : y)) : y;
   const float wyp = (c.pery || y + 1 < c.ny) ? 1.f : 0.f, wym = (c.pery || y - 1 >= 0) ? 1.f : 0.f;
   const float wzu = above ? 1.f : 0.f, wzd = below ? 1.f : 0.f;
-  const int xs[2] = {x, x + 2};
-  int xw[2];
-#pragma unroll
-  for (int s = 0; s < 2; s++) xw[s] = c.perx ? (xs[s] < 0 ? xs[s] + c.nx : (xs[s] >= c.nx ? xs[s] - c.nx : xs[s])) : xs[s];
-  Draw d[2];
+  const int xs1 = x + 2;
+  int xw0 = x, xw1 = xs1;
+  if (c.perx) {
+    xw0 = x < 0 ? x + c.nx : (x >= c.nx ? x - c.nx : x);
+    xw1 = xs1 < 0 ? xs1 + c.nx : (xs1 >= c.nx ? xs1 - c.nx : xs1);
+  }
+  Draw d0, d1;
   if (FLIP) {
-#pragma unroll
-    for (int s = 0; s < 2; s++) d[s] = site_draw(c.seed, c.sweep, xw[s], yw, zw, c.nx, c.ny, true);
+    d0 = site_draw(c.seed, c.sweep, xw0, yw, zw, c.nx, c.ny, true);
+    d1 = site_draw(c.seed, c.sweep, xw1, yw, zw, c.nx, c.ny, true);
   } else {
     // one Philox call serves both sites (x & ~2 is shared) unless a periodic wrap split a ring pair
-    const U4 out = site_draws(c.seed, c.sweep, pair_counter(xw[v0 ? 0 : 1], yw, zw, c.nx, c.ny), 0);
-    d[0] = pair_half(out, (xw[0] >> 1) & 1u);
-    d[1] = pair_half(out, (xw[1] >> 1) & 1u);
+    const U4 out = site_draws(c.seed, c.sweep, pair_counter(v0 ? xw0 : xw1, yw, zw, c.nx, c.ny), 0);
+    d0 = pair_half(out, (xw0 >> 1) & 1u);
+    d1 = pair_half(out, (xw1 >> 1) & 1u);
   }
-  SiteResult r[2];
-#pragma unroll
-  for (int s = 0; s < 2; s++) {
-    const Vec3 n = s == 0 ? Vec3{o[0].x, o[1].x, o[2].x} : Vec3{o[0].y, o[1].y, o[2].y};
-    Vec3 nb[6];
-    nb[0] = s == 0 ? Vec3{xb[0], xb[1], xb[2]} : Vec3{xc[0], xc[1], xc[2]};  // +x
-    nb[1] = s == 0 ? Vec3{xa[0], xa[1], xa[2]} : Vec3{xb[0], xb[1], xb[2]};  // -x
-    nb[2] = s == 0 ? Vec3{yu[0].x, yu[1].x, yu[2].x} : Vec3{yu[0].y, yu[1].y, yu[2].y};
-    nb[3] = s == 0 ? Vec3{yd[0].x, yd[1].x, yd[2].x} : Vec3{yd[0].y, yd[1].y, yd[2].y};
-    nb[4] = s == 0 ? Vec3{pu[0].x, pu[1].x, pu[2].x} : Vec3{pu[0].y, pu[1].y, pu[2].y};
-    nb[5] = s == 0 ? Vec3{pd[0].x, pd[1].x, pd[2].x} : Vec3{pd[0].y, pd[1].y, pd[2].y};
-    const float w[6] = {(c.perx || xs[s] + 1 < c.nx) ? 1.f : 0.f, (c.perx || xs[s] - 1 >= 0) ? 1.f : 0.f, wyp, wym, wzu,
-                        wzd};
-    r[s] = site_update<POT, FLIP>(m, n, nb, w, sid, sn, c.elecE, d[s], c.av, c.T, c.invT);
+  const LaneDraw<float2> ld = lane_draw(d0, d1, FLIP);
+  // lane 0: site x, lane 1: site x + 2
+  const V3<float2> n{o[0], o[1], o[2]};
+  const V3<float2> nb[6] = {
+      V3<float2>{make_float2(xb[0], xc[0]), make_float2(xb[1], xc[1]), make_float2(xb[2], xc[2])},  // +x
+      V3<float2>{make_float2(xa[0], xb[0]), make_float2(xa[1], xb[1]), make_float2(xa[2], xb[2])},  // -x
+      V3<float2>{yu[0], yu[1], yu[2]},
+      V3<float2>{yd[0], yd[1], yd[2]},
+      V3<float2>{pu[0], pu[1], pu[2]},
+      V3<float2>{pd[0], pd[1], pd[2]}};
+  float2 wxp = make_float2(1.f, 1.f), wxm = make_float2(1.f, 1.f);
+  if (!c.perx) {
+    wxp = make_float2(x + 1 < c.nx ? 1.f : 0.f, xs1 + 1 < c.nx ? 1.f : 0.f);
+    wxm = make_float2(x - 1 >= 0 ? 1.f : 0.f, xs1 - 1 >= 0 ? 1.f : 0.f);
   }
+  const float2 w[6] = {wxp, wxm, make_float2(wyp, wyp), make_float2(wym, wym), make_float2(wzu, wzu),
+                       make_float2(wzd, wzd)};
+  const SiteResultT<float2> r = site_update<POT, FLIP, float2>(m, n, nb, w, sid, sn, c.elecE, ld, c.av, c.T, c.invT);
   if (v0 | v1) {
+    const float2 nx2[3] = {r.n.x, r.n.y, r.n.z};
 #pragma unroll
     for (int q = 0; q < 3; q++) {
-      float2 v = o[q];
-      if (v0) v.x = q == 0 ? r[0].n.x : (q == 1 ? r[0].n.y : r[0].n.z);
-      if (v1) v.y = q == 0 ? r[1].n.x : (q == 1 ? r[1].n.y : r[1].n.z);
+      const float2 v = make_float2(v0 ? nx2[q].x : o[q].x, v1 ? nx2[q].y : o[q].y);
       *reinterpret_cast<float2 *>(own + q * PF) = v;
     }
   }
-  if (count) accepted += (v0 ? r[0].rot : 0u) + (v1 ? r[1].rot : 0u);
+  if (count) accepted += (v0 && r.rot.x ? 1u : 0u) + (v1 && r.rot.y ? 1u : 0u);
   if (meas) {
-    if (v0) e_acc += fmaf(2.f, r[0].bond, r[0].single);
-    if (v1) e_acc += fmaf(2.f, r[1].bond, r[1].single);
+    const float2 eb = __ffma2_rn(make_float2(2.f, 2.f), r.bond, r.single);
+    if (v0) e_acc += eb.x;
+    if (v1) e_acc += eb.y;
   }
 }
 
