@@ -22,7 +22,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
           "-I" + os.path.join(HERE, "..", "include")] + ARCH
 PER_FILE = {"kernels_ref8.cu": ["-fmad=false"]}
-SOURCES = ["kernels.cu", "kernels_ref8.cu", "sweep_fused.cu", "engine.cpp", "driver.cpp"]
+SOURCES = ["kernels.cu", "kernels_ref8.cu", "sweep_fused.cu", "sweep_fused_ll.cu", "sweep_fused_ghrl.cu",
+           "sweep_fused_pear.cu", "engine.cpp", "driver.cpp"]
 
 
 def nvcc():

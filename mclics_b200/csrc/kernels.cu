@@ -43,8 +43,8 @@ __global__ void __launch_bounds__(kThreads) k_sweep_color(ModelDev m, const RepD
       const Draw d = site_draw(R.seed, *sweep_ctr, x, y, z, R.nx, R.ny, m.flip);
       const LaneDraw<float> ld = lane_draw(d, m.flip);
       const SiteResultT<float> r =
-          m.flip ? site_update<POT, true, float>(m, n, nb, w, sid, s, S.elecE, ld, S.ang_var, T, invT)
-                 : site_update<POT, false, float>(m, n, nb, w, sid, s, S.elecE, ld, S.ang_var, T, invT);
+          m.flip ? site_update<POT, true, false, true, true, float>(m, n, nb, w, sid, s, S.elecE, ld, S.ang_var, T, invT)
+                 : site_update<POT, false, false, true, true, float>(m, n, nb, w, sid, s, S.elecE, ld, S.ang_var, T, invT);
       accepted = r.rot ? 1u : 0u;
       if (r.rot || r.flip) {
         dir[dir_index(R, 0, x, y, z)] = r.n.x;

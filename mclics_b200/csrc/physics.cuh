@@ -83,8 +83,9 @@ __device__ __forceinline__ L ll_bond(const ModelDev &m, const V3<L> &x, const V3
   return mul_(splat<L>(-1.5f * m.A), mul_(b, b));
 }
 
-// GHRL with bond vector r = sign * e_axis, src/potential.cpp:40-56.
-template <int AXIS, typename L>
+// GHRL with bond vector r = sign * e_axis, src/potential.cpp:40-56. CHIRAL = false drops the sigma term, which
+// is exact for sigma = 0 (fma(0, c, u) == u).
+template <int AXIS, bool CHIRAL, typename L>
 __device__ __forceinline__ L ghrl_bond(const ModelDev &m, const V3<L> &x, const V3<L> &y, float sign) {
   const L ai = comp<AXIS>(x), aj = comp<AXIS>(y);  // a_i a_j and a^2 do not depend on the sign of r
   const L b = dot(x, y);
@@ -92,7 +93,7 @@ __device__ __forceinline__ L ghrl_bond(const ModelDev &m, const V3<L> &x, const 
   const L e1 = fma_(splat<L>(1.5f), fma_(ai, ai, mul_(aj, aj)), splat<L>(-1.f));
   L u = fma_(e1, fma_(splat<L>(m.rho), p2, splat<L>(m.lam)),
              fma_(splat<L>(m.mu), fma_(mul_(ai, aj), b, splat<L>(-1.f / 9.f)), mul_(splat<L>(m.nu), p2)));
-  if (m.sigma != 0.f) {
+  if (CHIRAL) {
     // c = r . (n_j x n_i)
     const L c = AXIS == 0 ? fma_(y.y, x.z, neg_(mul_(y.z, x.y)))
                           : (AXIS == 1 ? fma_(y.z, x.x, neg_(mul_(y.x, x.z))) : fma_(y.x, x.y, neg_(mul_(y.y, x.x))));
@@ -125,23 +126,49 @@ __device__ __forceinline__ L pear_bond(const ModelDev &m, const V3<L> &x, const 
   return fma_(mul_(splat<L>(-m.A), b), b, fma_(splat<L>(-m.B1), b, mul_(splat<L>(-0.25f * m.C), ps)));
 }
 
-template <int POT, int D, typename L>
+template <int POT, int D, bool CHIRAL, typename L>
 __device__ __forceinline__ L bond(const ModelDev &m, const V3<L> &x, const V3<L> &y) {
   if (POT == POT_LL) return ll_bond(m, x, y);
-  if (POT == POT_GHRL) return ghrl_bond<BondDir<D>::axis>(m, x, y, BondDir<D>::sign);
+  if (POT == POT_GHRL) return ghrl_bond<BondDir<D>::axis, CHIRAL>(m, x, y, BondDir<D>::sign);
   return pear_bond<BondDir<D>::axis>(m, x, y, BondDir<D>::sign);
 }
 
-// Sum over the six bonds with weights w[d] in {0, 1} (0: free edge or empty site).
-template <int POT, typename L>
+// Bond sums of one or two directors over the six bonds, with weights w[d] in {0, 1} (0: free edge or empty
+// site). PXY = true: the x and y neighbours are known to be present, their weights are not applied (exact: the
+// weight would be 1). The two-director form evaluates both in one pass, so each neighbour is used once.
+template <int POT, bool PXY, bool CHIRAL, int D, typename L>
+__device__ __forceinline__ L acc_bond(const ModelDev &m, const V3<L> &x, const V3<L> &y, const L &w, const L &e) {
+  const L u = bond<POT, D, CHIRAL>(m, x, y);
+  if (PXY && D < 4) return D == 0 ? u : add_(e, u);
+  return D == 0 ? mul_(w, u) : fma_(w, u, e);
+}
+
+template <int POT, bool PXY, bool CHIRAL, typename L>
 __device__ __forceinline__ L bond_sum(const ModelDev &m, const V3<L> &x, const V3<L> (&nb)[6], const L (&w)[6]) {
-  L e = mul_(w[0], bond<POT, 0>(m, x, nb[0]));
-  e = fma_(w[1], bond<POT, 1>(m, x, nb[1]), e);
-  e = fma_(w[2], bond<POT, 2>(m, x, nb[2]), e);
-  e = fma_(w[3], bond<POT, 3>(m, x, nb[3]), e);
-  e = fma_(w[4], bond<POT, 4>(m, x, nb[4]), e);
-  e = fma_(w[5], bond<POT, 5>(m, x, nb[5]), e);
+  L e = acc_bond<POT, PXY, CHIRAL, 0>(m, x, nb[0], w[0], w[0]);
+  e = acc_bond<POT, PXY, CHIRAL, 1>(m, x, nb[1], w[1], e);
+  e = acc_bond<POT, PXY, CHIRAL, 2>(m, x, nb[2], w[2], e);
+  e = acc_bond<POT, PXY, CHIRAL, 3>(m, x, nb[3], w[3], e);
+  e = acc_bond<POT, PXY, CHIRAL, 4>(m, x, nb[4], w[4], e);
+  e = acc_bond<POT, PXY, CHIRAL, 5>(m, x, nb[5], w[5], e);
   return e;
+}
+
+template <int POT, bool PXY, bool CHIRAL, typename L>
+__device__ __forceinline__ void bond_sum2(const ModelDev &m, const V3<L> &x, const V3<L> &x2, const V3<L> (&nb)[6],
+                                          const L (&w)[6], L &e1, L &e2) {
+  e1 = acc_bond<POT, PXY, CHIRAL, 0>(m, x, nb[0], w[0], w[0]);
+  e2 = acc_bond<POT, PXY, CHIRAL, 0>(m, x2, nb[0], w[0], w[0]);
+  e1 = acc_bond<POT, PXY, CHIRAL, 1>(m, x, nb[1], w[1], e1);
+  e2 = acc_bond<POT, PXY, CHIRAL, 1>(m, x2, nb[1], w[1], e2);
+  e1 = acc_bond<POT, PXY, CHIRAL, 2>(m, x, nb[2], w[2], e1);
+  e2 = acc_bond<POT, PXY, CHIRAL, 2>(m, x2, nb[2], w[2], e2);
+  e1 = acc_bond<POT, PXY, CHIRAL, 3>(m, x, nb[3], w[3], e1);
+  e2 = acc_bond<POT, PXY, CHIRAL, 3>(m, x2, nb[3], w[3], e2);
+  e1 = acc_bond<POT, PXY, CHIRAL, 4>(m, x, nb[4], w[4], e1);
+  e2 = acc_bond<POT, PXY, CHIRAL, 4>(m, x2, nb[4], w[4], e2);
+  e1 = acc_bond<POT, PXY, CHIRAL, 5>(m, x, nb[5], w[5], e1);
+  e2 = acc_bond<POT, PXY, CHIRAL, 5>(m, x2, nb[5], w[5], e2);
 }
 
 // Field, src/potential.cpp:59-63.
@@ -194,13 +221,16 @@ __device__ __forceinline__ float anchoring_energy(const ModelDev &m, int sid, co
   return 0.f;
 }
 
-// Single-site terms: anchoring (sid >= 0, the same surface for both lanes) and field.
+// Single-site terms: anchoring (sid >= 0, the same surface for both lanes) and, with FIELD, the field (FIELD is
+// false only when elecA = elecP = 0, where the reference adds no field term either).
+template <bool FIELD>
 __device__ __forceinline__ float single_energy(const ModelDev &m, const Vec3 &x, int sid, const Vec3 &s, float elecE) {
   float e = 0.f;
   if (sid >= 0) e = anchoring_energy(m, sid, x, s);
-  if (m.field_on) e = __fadd_rn(e, field_energy(m, x, elecE));
+  if (FIELD && m.field_on) e = __fadd_rn(e, field_energy(m, x, elecE));
   return e;
 }
+template <bool FIELD>
 __device__ __forceinline__ float2 single_energy(const ModelDev &m, const V3<float2> &x, int sid, const Vec3 &s,
                                                 float elecE) {
   float2 e = make_float2(0.f, 0.f);
@@ -208,7 +238,7 @@ __device__ __forceinline__ float2 single_energy(const ModelDev &m, const V3<floa
     e.x = anchoring_energy(m, sid, Vec3{x.x.x, x.y.x, x.z.x}, s);
     e.y = anchoring_energy(m, sid, Vec3{x.x.y, x.y.y, x.z.y}, s);
   }
-  if (m.field_on) e = __fadd2_rn(e, field_energy(m, x, elecE));
+  if (FIELD && m.field_on) e = __fadd2_rn(e, field_energy(m, x, elecE));
   return e;
 }
 
@@ -284,14 +314,17 @@ __device__ __forceinline__ V3<L> sel3(LB<L> c, const V3<L> &a, const V3<L> &b) {
 }
 
 // One trial move (src/evolve.cpp:133-207): rotation, Metropolis, then the optional n -> -n trial.
-template <int POT, bool FLIP, typename L>
+// Compile-time features: FLIP (n -> -n trial), PXY (x, y neighbours always present), CHIRAL (GHRL sigma term),
+// FIELD (field term). Every combination rounds like the general one on the inputs it applies to.
+template <int POT, bool FLIP, bool PXY, bool CHIRAL, bool FIELD, typename L>
 __device__ __forceinline__ SiteResultT<L> site_update(const ModelDev &m, const V3<L> &n, const V3<L> (&nb)[6],
                                                       const L (&w)[6], int sid, const Vec3 &s, float elecE,
                                                       const LaneDraw<L> &d, float av, float T, float invT) {
   const L va = mul_(fma_(splat<L>(2.f), d.u1, splat<L>(-1.f)), splat<L>(av));
   const V3<L> nn = rotate_trial(n, va, d.w0, d.w1, d.w2);
-  const L b_old = bond_sum<POT>(m, n, nb, w), b_new = bond_sum<POT>(m, nn, nb, w);
-  const L s_old = single_energy(m, n, sid, s, elecE), s_new = single_energy(m, nn, sid, s, elecE);
+  L b_old, b_new;
+  bond_sum2<POT, PXY, CHIRAL>(m, n, nn, nb, w, b_old, b_new);
+  const L s_old = single_energy<FIELD>(m, n, sid, s, elecE), s_new = single_energy<FIELD>(m, nn, sid, s, elecE);
   const L e_old = add_(b_old, s_old), e_new = add_(b_new, s_new);
   SiteResultT<L> r;
   r.rot = metropolis(d.u3, sub_(e_new, e_old), invT, T);
@@ -300,7 +333,7 @@ __device__ __forceinline__ SiteResultT<L> site_update(const ModelDev &m, const V
   r.single = sel_(r.rot, s_new, s_old);
   if (FLIP) {
     const V3<L> f{neg_(r.n.x), neg_(r.n.y), neg_(r.n.z)};
-    const L bf = bond_sum<POT>(m, f, nb, w), sf = single_energy(m, f, sid, s, elecE);
+    const L bf = bond_sum<POT, PXY, CHIRAL>(m, f, nb, w), sf = single_energy<FIELD>(m, f, sid, s, elecE);
     const L e_cur = add_(r.bond, r.single);
     r.flip = metropolis(d.u4, sub_(add_(bf, sf), e_cur), invT, T);
     r.n = sel3<L>(r.flip, f, r.n);
@@ -316,7 +349,7 @@ __device__ __forceinline__ SiteResultT<L> site_update(const ModelDev &m, const V
 template <int POT>
 __device__ __forceinline__ float site_energy(const ModelDev &m, const Vec3 &x, const Vec3 (&nb)[6], const float (&w)[6],
                                              int sid, const Vec3 &s, float elecE) {
-  return __fadd_rn(bond_sum<POT>(m, x, nb, w), single_energy(m, x, sid, s, elecE));
+  return __fadd_rn(bond_sum<POT, false, true>(m, x, nb, w), single_energy<true>(m, x, sid, s, elecE));
 }
 
 }  // namespace mcl
