@@ -159,6 +159,27 @@ int mcl_debug_wait_limit(mcl_engine *e, long long timeout_ns, int withhold_first
  * director_field_*.csv. The mode may be given with or without the GPU suffix. */
 int mcl_run_input_file(const char *path);
 
+/* Observables of a bulk or slab lattice whose directors already lie in device memory, computed without allocating
+ * anything. No counterpart in the reference. mcl_measure needs an engine, and mcl_create allocates the engine's
+ * buffers; this function serves callers that hold the directors in their own device buffer and cannot allocate
+ * when they measure, such as a program whose pool allocator has reserved the device's memory, or a loop that
+ * must not absorb the device-wide synchronisation of cudaMalloc/cudaFree.
+ *   d_ni     3 floats per site, site (i, j, k) at index i + Nx (j + Ny k), in memory of the current device (or
+ *            managed memory); its allocation must hold all 3 Nx Ny Nz floats (checked).
+ *   out      host struct: energy, q, S, director, nsum and n_valid as mcl_measure gives them (within FP64
+ *            rounding of the sums); acceptance 0, ang_var = replica->ang_var, sweep 0. replica->T and seed are
+ *            not used.
+ *   stream   cudaStream_t the two kernels run on (NULL: the default stream); the call waits for that stream.
+ * Limits: at most 2^26 = 67,108,864 sites; larger lattices return MCL_ERR_ARG (the partial sums go to a fixed
+ * 1.25 MiB array in the library's device memory). Sphere and custom geometries return MCL_ERR_ARG.
+ * The first call on each device looks up that array's address (cudaGetSymbolAddress), which may load the
+ * library's device code; make that first call before any stream capture on the device. The device must not be
+ * reset (cudaDeviceReset) afterwards. Nothing in the array needs to start at zero. There is one array per device:
+ * calls on the same device must not overlap (from several host threads, or on several streams); they would
+ * overwrite each other's partial sums. */
+int mcl_observe_device(const mcl_model *model, const mcl_replica *replica, const float *d_ni, mcl_observables *out,
+                       void *stream);
+
 /* Message of the last failed call on this thread ("" if none). */
 const char *mcl_last_error(void);
 /* Library version string. */
