@@ -127,30 +127,69 @@ def ncu_traffic(kernel_key):
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle samples while the timed region runs."""
+    """SM clock and clock-event reasons of this rank's GPU, sampled every 10 ms through NVML while the timed
+    regions run (nvidia-smi every 200 ms when NVML is unavailable). The GPU is found by the UUID torch reports,
+    so CUDA_VISIBLE_DEVICES reordering does not matter."""
 
+    REASONS = [("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4), ("hw_power_brake_slowdown", 0x80)]
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index):
         self.index = index
-        self.samples = []
+        self.samples = []  # (sm_mhz, max_mhz, set of reason names)
+        self.source = None
         self._stop = threading.Event()
         self._t = None
+        self._nvml = None
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            uuid = str(torch.cuda.get_device_properties(index).uuid)
+            try:
+                h = pynvml.nvmlDeviceGetHandleByUUID(("GPU-" + uuid).encode())
+            except Exception:
+                h = pynvml.nvmlDeviceGetHandleByUUID("GPU-" + uuid)
+            self._nvml = (pynvml, h, pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+            self.source = "nvml"
+        except Exception:
+            self._nvml = None
+            self.source = "nvidia-smi"
+
+    def _sample(self):
+        if self._nvml:
+            nv, h, mx = self._nvml
+            sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+            try:
+                bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+            except Exception:
+                bits = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+            self.samples.append((float(sm), float(mx), {n for n, b in self.REASONS if bits & b}))
+            return 0.01
+        out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                              "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                             timeout=5).stdout.strip()
+        if out:
+            s = [x.strip() for x in out.split(",")]
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            rs = {n for k, n in enumerate(names) if len(s) > 5 + k and s[5 + k].lower().startswith("active")}
+            if s[1].replace(".", "").isdigit() and s[2].replace(".", "").isdigit():
+                self.samples.append((float(s[1]), float(s[2]), rs))
+        return 0.2
 
     def start(self):
+        self._stop.clear()
+
         def loop():
             while not self._stop.is_set():
                 try:
-                    out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
-                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
-                                         timeout=5).stdout.strip()
-                    if out:
-                        self.samples.append([x.strip() for x in out.split(",")])
+                    dt = self._sample()
                 except Exception:
-                    pass
-                self._stop.wait(0.2)
+                    dt = 0.2
+                self._stop.wait(dt)
         self._t = threading.Thread(target=loop, daemon=True)
         self._t.start()
 
@@ -161,17 +200,15 @@ class ClockSampler:
 
     def summary(self):
         if not self.samples:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
-        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0,
+                    "source": self.source}
         reasons = set()
         for s in self.samples:
-            for k, name in enumerate(names):
-                if len(s) > 5 + k and s[5 + k].lower().startswith("active"):
-                    reasons.add(name)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.samples)}
+            reasons |= s[2]
+        return {"sm_mhz": statistics.median(s[0] for s in self.samples),
+                "sm_max_mhz": max(s[1] for s in self.samples), "reasons": sorted(reasons),
+                "samples": len(self.samples), "source": self.source,
+                "region": "device-timed and end-to-end-timed steps"}
 
 
 def reference_cpu(steps, warmup, budget_s=150.0):
@@ -252,6 +289,7 @@ def gpu_arm(args, rank, world, local_rank):
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
+    clocks.start()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         for i in range(len(reps)):
@@ -261,6 +299,7 @@ def gpu_arm(args, rank, world, local_rank):
             eng.series(i, eng.series_length() - 1, 1)
             M.check(M.lib().mcl_download_directors(eng._h, i, host_ni[i].data_ptr()))
     e2e_s = time.perf_counter() - t0
+    clocks.stop()
 
     times = torch.tensor([dev_ms, e2e_s * 1e3], dtype=torch.float64, device=dev)
     if world > 1:
@@ -275,8 +314,8 @@ def gpu_arm(args, rank, world, local_rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="mclics_b200", choices=["mclics_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"],
@@ -288,7 +327,7 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     _, _, config, _ = workload(args.workload) if args.impl != "reference" else workload("c2")
-    config = dict(config, step="1 sweep + measurement of every lattice",
+    config = dict(config, step="1 sweep + measurement of every lattice", accumulators="f64 (energy, Q, sum n)",
                   parallelism="independent replicas x%d" % max(1, args.gpus))
 
     if args.impl == "reference":
@@ -301,7 +340,7 @@ def main():
         v = r["sites"] * r["steps"] / r["seconds"]
         line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "site-updates/s", "n_gpus": args.gpus,
                 "steps": r["steps"], "warmup": args.warmup, "ms_per_step": 1e3 * r["seconds"] / r["steps"],
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 accumulators)",
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic", "config": config,
                 "cpu_baseline": {"value": v, "unit": "site-updates/s", "cores": r["threads"], "kind": "reference",
                                  "sample": "%d measured sweeps of the 256^3 lattice after %d warm-up (reference "
@@ -343,8 +382,8 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": "site-updates/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": res["dev_ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32 (f64 accumulators)", "data": "synthetic", "config": config,
-        "e2e": {"value": e2e, "unit": "site-updates/s", "h2d_bytes_per_step": 4,
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config,
+        "e2e": {"value": e2e, "unit": "site-updates/s", "h2d_bytes_per_step": 4 * res["n_rep"],
                 "d2h_bytes_per_step": 144 * res["n_rep"] + 12 * res["sites"]},
         "gpu_launches": res["launches"],
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
