@@ -159,6 +159,54 @@ int mcl_debug_wait_limit(mcl_engine *e, long long timeout_ns, int withhold_first
  * director_field_*.csv. The mode may be given with or without the GPU suffix. */
 int mcl_run_input_file(const char *path);
 
+/* ---- Learned Metropolis-Hastings proposal (no counterpart in the reference) ----------------------------------
+ * Per site, a 7 -> 64 -> 64 -> 4 MLP with SiLU reads the neighbour Q-tensor sum sum_j (3 n_j n_j^T - I)/2 divided by
+ * 6 (xx, xy, xz, yy, yz, zz) and T, and gives an axis mu (outputs 0..2, normalised) and a concentration
+ * kappa = clip(softplus(output 3), 1e-3, kappa_max). The trial director is drawn from
+ *   q(n) = [0.95 kappa cosh(kappa mu.n) / sinh(kappa) + 0.05] / (4 pi)
+ * (antipodally symmetrised von Mises-Fisher plus 5 % uniform) and accepted with probability
+ * min(1, exp(-dE/T) q(n_old) / q(n_new)); q does not depend on the site's own director, so the Boltzmann
+ * distribution stays exact for any weights. Weights and hidden activations are rounded to BF16, sums are FP32. */
+typedef struct mcl_mlp {
+  float w1[64][7]; /* [out][in] */
+  float b1[64];
+  float w2[64][64];
+  float b2[64];
+  float w3[4][64];
+  float b3[4];
+} mcl_mlp;
+
+/* Sweeps of this engine use the learned proposal with these weights (copied; NULL returns to the plain
+ * proposal). While it is set, ang_var is not adapted and the acceptance in the series is that of the learned
+ * moves. Every site gets one learned trial per sweep, colour by colour (no separate n -> -n trial: the proposal is
+ * symmetric under n -> -n). */
+int mcl_set_proposal(mcl_engine *e, const mcl_mlp *mlp, float kappa_max);
+/* ang_var adaptation after each sweep (default 1, as the reference). 0 keeps the plain proposal's amplitude fixed,
+ * the fixed-amplitude judge of autocorrelation comparisons. */
+int mcl_set_adaptation(mcl_engine *e, int enable);
+/* Training samples from the current state of one replica: n sites drawn with Philox(seed, sample index). Device
+ * buffers: d_features n x 8 floats (7 features, then 1 for a non-empty site / 0 for an empty one), d_directors
+ * n x 3 floats (the site's director). Synchronises. */
+int mcl_extract_samples(mcl_engine *e, int replica, long long n, unsigned long long seed, float *d_features,
+                        float *d_directors);
+/* The tensor-core MLP on n feature rows (device, n x 8 floats as above) -> d_out n x 4 raw outputs (before the
+ * normalisation of mu and the softplus of kappa). Synchronises `stream`. */
+int mcl_mlp_forward(const mcl_mlp *mlp, const float *d_features, long long n, float *d_out, void *stream);
+
+/* Training on the GPU: loss = -mean log(4 pi q(n | features)) over samples (maximum likelihood of the site's
+ * conditional distribution), Adam (beta 0.9 / 0.999, eps 1e-8) on FP32 master weights, BF16-rounded weights in
+ * the passes. Batches are device buffers in the mcl_extract_samples format, at most max_batch rows. */
+typedef struct mcl_trainer mcl_trainer;
+int mcl_trainer_create(const mcl_mlp *init, long long max_batch, float kappa_max, mcl_trainer **out);
+/* Gradient of the mean loss at the current weights (no update) and the loss. Synchronises. */
+int mcl_trainer_gradient(mcl_trainer *t, const float *d_features, const float *d_directors, long long n,
+                         mcl_mlp *grad, double *loss);
+/* One Adam step with learning rate lr; loss (may be NULL) is the batch loss before the step. */
+int mcl_trainer_step(mcl_trainer *t, const float *d_features, const float *d_directors, long long n, float lr,
+                     double *loss);
+int mcl_trainer_get(mcl_trainer *t, mcl_mlp *out);
+int mcl_trainer_destroy(mcl_trainer *t);
+
 /* Observables of a bulk or slab lattice whose directors already lie in device memory, computed without allocating
  * anything. No counterpart in the reference. mcl_measure needs an engine, and mcl_create allocates the engine's
  * buffers; this function serves callers that hold the directors in their own device buffer and cannot allocate

@@ -24,6 +24,8 @@ GEOMETRIES = {"bulk": 0, "slab": 1, "sphere": 2, "custom": 3}
 ANCHORINGS = {"homeotropic": 0, "rp": 1, "rp_tangent": 2, "fg": 3, "homeotropic_ghrl": 4, "rp_ghrl": 5,
               "fg_ghrl": 6}
 SCHED_REF8, SCHED_CHECKER2, SCHED_CHECKER2_SIMPLE = 0, 1, 2
+N_MLP_PARAMS = 64 * 7 + 64 + 64 * 64 + 64 + 4 * 64 + 4  # learned proposal network 7 -> 64 -> 64 -> 4
+KAPPA_MAX = 500.0
 STATUS = {0: "MCL_OK", 1: "MCL_ERR_ARG", 2: "MCL_ERR_CUDA", 3: "MCL_ERR_NOMEM", 4: "MCL_ERR_STATE",
           5: "MCL_ERR_INPUT", 6: "MCL_ERR_IO", 7: "MCL_ERR_NONFINITE", 8: "MCL_ERR_NO_DEVICE"}
 
@@ -96,6 +98,15 @@ def lib():
             "mcl_profile": [vp, i],
             "mcl_debug_wait_limit": [vp, ctypes.c_longlong, i],
             "mcl_profile_read": [vp, P(ctypes.c_double), P(ctypes.c_longlong), P(ctypes.c_longlong)],
+            "mcl_set_proposal": [vp, vp, f],
+            "mcl_set_adaptation": [vp, i],
+            "mcl_extract_samples": [vp, i, ctypes.c_longlong, ctypes.c_ulonglong, vp, vp],
+            "mcl_mlp_forward": [vp, vp, ctypes.c_longlong, vp, vp],
+            "mcl_trainer_create": [vp, ctypes.c_longlong, f, P(vp)],
+            "mcl_trainer_gradient": [vp, vp, vp, ctypes.c_longlong, vp, P(ctypes.c_double)],
+            "mcl_trainer_step": [vp, vp, vp, ctypes.c_longlong, f, P(ctypes.c_double)],
+            "mcl_trainer_get": [vp, vp],
+            "mcl_trainer_destroy": [vp],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -290,6 +301,75 @@ class Engine:
         out = np.empty(self.sites(r), np.uint8)
         check(lib().mcl_read_decisions(self._h, r, out.ctypes.data))
         return out
+
+    def set_proposal(self, params=None, kappa_max=KAPPA_MAX):
+        """Learned proposal with the flat MLP parameter vector `params` (N_MLP_PARAMS floats, mcl_mlp order);
+        None returns to the plain proposal."""
+        if params is None:
+            check(lib().mcl_set_proposal(self._h, None, kappa_max))
+            return
+        p = mlp_params(params)
+        check(lib().mcl_set_proposal(self._h, p.ctypes.data, kappa_max))
+
+    def set_adaptation(self, on=True):
+        check(lib().mcl_set_adaptation(self._h, 1 if on else 0))
+
+    def extract_samples(self, r, n, seed, features_ptr, directors_ptr):
+        """n training samples of replica r into device buffers (n x 8 and n x 3 floats)."""
+        check(lib().mcl_extract_samples(self._h, r, n, seed, ctypes.c_void_p(features_ptr),
+                                        ctypes.c_void_p(directors_ptr)))
+
+
+def mlp_params(params):
+    p = np.ascontiguousarray(params, np.float32).reshape(-1)
+    if p.size != N_MLP_PARAMS:
+        raise ValueError("the MLP has %d parameters, got %d" % (N_MLP_PARAMS, p.size))
+    return p
+
+
+def mlp_forward(params, features_ptr, n, out_ptr, stream=0):
+    """Raw network outputs (n x 4) of the tensor-core MLP for n device feature rows (n x 8)."""
+    p = mlp_params(params)
+    check(lib().mcl_mlp_forward(p.ctypes.data, ctypes.c_void_p(features_ptr), n, ctypes.c_void_p(out_ptr),
+                                ctypes.c_void_p(stream or 0)))
+
+
+class Trainer:
+    """GPU training of the proposal network (mcl_trainer_*): maximum likelihood, Adam."""
+
+    def __init__(self, params, max_batch, kappa_max=KAPPA_MAX):
+        self._h = ctypes.c_void_p()
+        p = mlp_params(params)
+        check(lib().mcl_trainer_create(p.ctypes.data, max_batch, kappa_max, ctypes.byref(self._h)))
+
+    def gradient(self, features_ptr, directors_ptr, n):
+        g = np.empty(N_MLP_PARAMS, np.float32)
+        loss = ctypes.c_double()
+        check(lib().mcl_trainer_gradient(self._h, ctypes.c_void_p(features_ptr), ctypes.c_void_p(directors_ptr), n,
+                                         g.ctypes.data, ctypes.byref(loss)))
+        return loss.value, g
+
+    def step(self, features_ptr, directors_ptr, n, lr):
+        loss = ctypes.c_double()
+        check(lib().mcl_trainer_step(self._h, ctypes.c_void_p(features_ptr), ctypes.c_void_p(directors_ptr), n, lr,
+                                     ctypes.byref(loss)))
+        return loss.value
+
+    def params(self):
+        p = np.empty(N_MLP_PARAMS, np.float32)
+        check(lib().mcl_trainer_get(self._h, p.ctypes.data))
+        return p
+
+    def close(self):
+        if self._h:
+            lib().mcl_trainer_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def run_input_file(path):

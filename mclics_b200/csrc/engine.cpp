@@ -353,6 +353,7 @@ int mcl_destroy(mcl_engine *e) {
   free_table(e->sites);
   cudaFree(e->d_dir[0]);
   cudaFree(e->d_dir[1]);
+  cudaFree(e->d_mlp);
   cudaFree(e->d_pt);
   cudaFree(e->d_nrm);
   cudaFree(e->d_stage);
@@ -493,7 +494,7 @@ int mcl_sweeps(mcl_engine *e, int n, int measure) {
   if (n == 0) return MCL_OK;
   int rc;
   if (measure && (rc = ensure_series(e, e->series_len + n))) return rc;
-  const bool use_fused = e->fused && !e->record_dec;
+  const bool use_fused = e->fused && !e->record_dec && !e->d_mlp;
   if (use_fused && (rc = refresh_ghosts(e))) return rc;
   for (int s = 0; s < n; s++) {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -512,7 +513,10 @@ int mcl_sweeps(mcl_engine *e, int n, int measure) {
     } else {
       LaunchCtx c = e->ctx();
       if (ev0) CK(cudaEventRecord(ev0, e->stream));
-      if (e->schedule == MCL_SCHED_REF8) {
+      if (e->d_mlp) {
+        CK(launch_sweep_learned(c, e->geo, e->half, e->d_mlp, e->kappa_max));
+        e->launches += 2;
+      } else if (e->schedule == MCL_SCHED_REF8) {
         CK(launch_sweep_ref8(c, e->geo, e->boxes));
         e->launches += 8;
       } else {

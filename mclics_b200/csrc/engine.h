@@ -16,6 +16,7 @@ int fail(int code, const char *fmt, ...);
 int cuda_fail(cudaError_t err, const char *what);
 
 struct FusedPlan;  // fused tiled sweep (sweep_fused.cu)
+struct MlpDev;     // learned proposal weights in device layout (learned.cu)
 
 }  // namespace mcl
 
@@ -64,6 +65,9 @@ struct mcl_engine {
   double prof_ms = 0;          // time of already-read event pairs
   long long prof_sweeps = 0;
   long long launches = 0;      // kernels launched by this engine
+  mcl::MlpDev *d_mlp = nullptr;  // learned proposal (null: plain proposal)
+  float kappa_max = 500.f;
+  bool adapt = true;           // ang_var adaptation after each sweep (the reference's behaviour)
 
   mcl::LaunchCtx ctx() const {
     mcl::LaunchCtx c;
@@ -77,6 +81,7 @@ struct mcl_engine {
     c.sweep_ctr = d_sweep;
     c.decisions = record_dec ? d_dec : nullptr;
     c.stream = stream;
+    c.adapt = (adapt && !d_mlp) ? 1 : 0;
     return c;
   }
 };

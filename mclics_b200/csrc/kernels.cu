@@ -117,7 +117,8 @@ __global__ void __launch_bounds__(kThreads) k_observe(ModelDev m, const RepDesc 
 
 // ------------------------------------------------------------------------------------------------------------
 // One block per replica: deterministic reduction of the replica's partials, S and director by Jacobi, ang_var
-// adaptation (src/evolve.cpp:211-220), optional series record, reset of the acceptance counter. The last
+// adaptation (src/evolve.cpp:211-220; skipped when adapt = 0), optional series record, reset of the acceptance
+// counter. The last
 // block to finish advances the global sweep counter and the series length. measure: 0 none, 1 append to the
 // series, 2 probe (record the current state into series[rep]; no adaptation, counters untouched).
 __global__ void __launch_bounds__(kThreads) k_finalize(const RepDesc *__restrict__ reps, RepState *__restrict__ st,
@@ -125,7 +126,8 @@ __global__ void __launch_bounds__(kThreads) k_finalize(const RepDesc *__restrict
                                                        const double *__restrict__ partials, int measure,
                                                        ObsRecord *__restrict__ series, int *__restrict__ series_len,
                                                        unsigned long long *__restrict__ sweep_ctr,
-                                                       unsigned int *__restrict__ done_ctr, int n_replicas) {
+                                                       unsigned int *__restrict__ done_ctr, int n_replicas,
+                                                       int adapt) {
   const int rep = blockIdx.x;
   __shared__ double red[kThreads / 32][kPartials];
   __shared__ double tot[kPartials];
@@ -161,7 +163,8 @@ __global__ void __launch_bounds__(kThreads) k_finalize(const RepDesc *__restrict
     float av = S.ang_var;
     if (!probe) {
       a = (double)S.acc / nv;
-      if (1.0 * (double)S.acc / nv < 0.5) {
+      if (!adapt) {
+      } else if (1.0 * (double)S.acc / nv < 0.5) {
         av = (float)((double)av * 0.99);
         if (av < 0.01) av = 0.01f;
       } else if (1.0 * (double)S.acc / nv > 0.5) {
@@ -325,7 +328,7 @@ cudaError_t launch_observe(const LaunchCtx &c, int geo, const BlockTable &sites,
 cudaError_t launch_finalize(const LaunchCtx &c, const BlockTable &sites, const double *partials, int measure,
                             ObsRecord *series, int *series_len, unsigned int *done_ctr) {
   k_finalize<<<c.n_replicas, kThreads, 0, c.stream>>>(c.reps, c.state, sites.first, partials, measure, series,
-                                                       series_len, c.sweep_ctr, done_ctr, c.n_replicas);
+                                                       series_len, c.sweep_ctr, done_ctr, c.n_replicas, c.adapt);
   return cudaGetLastError();
 }
 

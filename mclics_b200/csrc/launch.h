@@ -26,6 +26,7 @@ struct LaunchCtx {
   unsigned long long *sweep_ctr;  // device
   uint8_t *decisions;       // device, null unless recording
   cudaStream_t stream;
+  int adapt = 1;            // ang_var adaptation after each sweep (off: the amplitude stays fixed)
 };
 
 constexpr int kThreads = 256;
@@ -41,6 +42,10 @@ cudaError_t launch_finalize(const LaunchCtx &c, const BlockTable &sites, const d
                             ObsRecord *series, int *series_len, unsigned int *done_ctr);
 // Periodic ghost cells (x then y) of every replica.
 cudaError_t launch_refresh_ghosts(const LaunchCtx &c, int max_ny_nz, int max_px_nz);
+// One sweep with the learned proposal (two colours, in place); mlp: weights in device layout (learned.cu).
+struct MlpDev;
+cudaError_t launch_sweep_learned(const LaunchCtx &c, int geo, const BlockTable &half, const MlpDev *mlp,
+                                 float kappa_max);
 // AoS (reference layout) <-> padded SoA for one replica.
 cudaError_t launch_unpack(const LaunchCtx &c, int replica, const RepDesc &host_desc, const float *aos);
 cudaError_t launch_pack(const LaunchCtx &c, int replica, const RepDesc &host_desc, float *aos);

@@ -1,0 +1,812 @@
+// Learned Metropolis-Hastings proposal (no counterpart in the reference).
+//
+// Per site the proposal reads only the neighbours: the features are the neighbour Q-tensor sum
+// sum_j w_j (3 n_j n_j^T - I) / 2, divided by 6 (xx, xy, xz, yy, yz, zz), and T. A 7 -> 64 -> 64 -> 4 MLP with SiLU
+// maps them to an axis mu (first three outputs, normalised) and a concentration kappa = clip(softplus(o_3),
+// 1e-3, kappa_max). The proposal density is
+//     q(n) = [ 0.95 kappa cosh(kappa mu.n) / sinh(kappa) + 0.05 ] / (4 pi),
+// an antipodally symmetrised von Mises-Fisher density mixed with 5 % uniform; it is sampled exactly (Wood's method
+// for the vMF part, a random sign, or a uniform point). Because q does not depend on the site's own director, the
+// Hastings test u < exp(-dE / T) q(n_old) / q(n_new) leaves the Boltzmann distribution invariant for any weights.
+//
+// The MLP runs on the tensor cores: one warp evaluates 32 sites as two 16-row tiles with mma.sync m16n8k16
+// (BF16 operands, FP32 accumulation); the FP32 accumulator fragments of one layer, after bias and SiLU, are packed
+// to BF16 and used directly as the A fragments of the next layer. Weights live in shared memory, rows padded so
+// that the fragment loads are free of bank conflicts.
+//
+// Training (maximum likelihood of the local conditional distribution, loss -log(4 pi q(n | features)) over sites
+// of equilibrated plain-sweep states) runs in FP32 on the CUDA cores with the same BF16 rounding of weights,
+// features and hidden activations as inference: one thread per sample for the forward and backward passes, then
+// the block's weight gradients from its 64 samples in shared memory, per-block partial sums, and a fixed-order
+// FP64 reduction with the Adam update.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+#include "engine.h"
+#include "launch.h"
+#include "physics.cuh"
+#include "site_access.cuh"
+
+namespace mcl {
+
+constexpr int kIn = 7, kH = 64, kOut = 4;
+constexpr int kNP = kH * kIn + kH + kH * kH + kH + kOut * kH + kOut;  // 4932 parameters
+constexpr int oW1 = 0, oB1 = oW1 + kH * kIn, oW2 = oB1 + kH, oB2 = oW2 + kH * kH, oW3 = oB2 + kH,
+              oB3 = oW3 + kOut * kH;
+static_assert(oB3 + kOut == kNP, "parameter layout");
+static_assert(sizeof(mcl_mlp) == kNP * sizeof(float), "mcl_mlp must be the flat parameter vector");
+constexpr float kEps = 0.05f, kKappaMin = 1e-3f;
+constexpr int kFeat = 8;  // floats per sample row: 7 features, validity flag
+
+// Weights in the layout of the tensor-core fragments: [n][k] rows (k contiguous), k padded with zeros (layer 1:
+// 7 -> 16), rows padded to 24 / 72 halves so that the 8 rows of a fragment load hit distinct banks; layer 3 has
+// 8 rows (4 used).
+struct MlpDev {
+  __nv_bfloat16 w1[kH][24];
+  __nv_bfloat16 w2[kH][72];
+  __nv_bfloat16 w3[8][72];
+  float b1[kH], b2[kH], b3[8];
+};
+static_assert(sizeof(MlpDev) % 16 == 0, "MlpDev is copied in 16-byte words");
+
+// ---- host: FP32 parameters -> device layout ------------------------------------------------------------------
+static uint16_t bf16_bits(float f) {  // round to nearest, ties to even
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  u = u + 0x7FFFu + ((u >> 16) & 1u);
+  return (uint16_t)(u >> 16);
+}
+
+static void set_bf16(__nv_bfloat16 *dst, float v) {
+  const uint16_t b = bf16_bits(v);
+  memcpy(dst, &b, 2);
+}
+
+static void to_device_layout(const mcl_mlp &p, MlpDev &d) {
+  memset(&d, 0, sizeof d);
+  const float *f = reinterpret_cast<const float *>(&p);
+  for (int n = 0; n < kH; n++) {
+    for (int k = 0; k < kIn; k++) set_bf16(&d.w1[n][k], f[oW1 + n * kIn + k]);
+    for (int k = 0; k < kH; k++) set_bf16(&d.w2[n][k], f[oW2 + n * kH + k]);
+    d.b1[n] = f[oB1 + n];
+    d.b2[n] = f[oB2 + n];
+  }
+  for (int n = 0; n < kOut; n++) {
+    for (int k = 0; k < kH; k++) set_bf16(&d.w3[n][k], f[oW3 + n * kH + k]);
+    d.b3[n] = f[oB3 + n];
+  }
+}
+
+// ---- device helpers ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ float sigm_f(float z) { return __fdividef(1.f, 1.f + __expf(-fmaxf(z, -80.f))); }
+__device__ __forceinline__ float silu_f(float z) { return z * sigm_f(z); }
+__device__ __forceinline__ float bf16r(float v) { return __bfloat162float(__float2bfloat16_rn(v)); }
+
+__device__ __forceinline__ uint32_t pack2(float lo, float hi) {
+  const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<const uint32_t *>(&v);
+}
+__device__ __forceinline__ uint32_t ld32(const __nv_bfloat16 *p) { return *reinterpret_cast<const uint32_t *>(p); }
+
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+      "{%0, %1, %2, %3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// Features of a site from its neighbours (weights w in {0, 1}) and T.
+__device__ __forceinline__ void site_features(const Vec3 (&nb)[6], const float (&w)[6], float T, float (&f)[kIn]) {
+  float mxx = 0.f, mxy = 0.f, mxz = 0.f, myy = 0.f, myz = 0.f, mzz = 0.f, k = 0.f;
+#pragma unroll
+  for (int d = 0; d < 6; d++) {
+    const float ax = w[d] * nb[d].x, ay = w[d] * nb[d].y, az = w[d] * nb[d].z;
+    mxx = fmaf(ax, nb[d].x, mxx);
+    mxy = fmaf(ax, nb[d].y, mxy);
+    mxz = fmaf(ax, nb[d].z, mxz);
+    myy = fmaf(ay, nb[d].y, myy);
+    myz = fmaf(ay, nb[d].z, myz);
+    mzz = fmaf(az, nb[d].z, mzz);
+    k += w[d];
+  }
+  const float c = 1.f / 6.f;
+  f[0] = fmaf(1.5f, mxx, -0.5f * k) * c;
+  f[1] = 1.5f * mxy * c;
+  f[2] = 1.5f * mxz * c;
+  f[3] = fmaf(1.5f, myy, -0.5f * k) * c;
+  f[4] = 1.5f * myz * c;
+  f[5] = fmaf(1.5f, mzz, -0.5f * k) * c;
+  f[6] = T;
+}
+
+// The MLP for the 32 sites of a warp (lane = site). All 32 lanes must call it (mma.sync is warp-wide). As / Out:
+// this warp's scratch in shared memory.
+__device__ __forceinline__ void warp_mlp(const MlpDev &S, __nv_bfloat16 (*As)[24], float (*Out)[4],
+                                         const float (&f)[kIn], float (&o)[kOut]) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  uint32_t *row = reinterpret_cast<uint32_t *>(As[lane]);
+  row[0] = pack2(f[0], f[1]);
+  row[1] = pack2(f[2], f[3]);
+  row[2] = pack2(f[4], f[5]);
+  row[3] = pack2(f[6], 0.f);
+  row[4] = row[5] = row[6] = row[7] = 0u;
+  __syncwarp();
+#pragma unroll 1
+  for (int mt = 0; mt < 2; mt++) {
+    const int r0 = 16 * mt + g, r1 = r0 + 8;
+    const uint32_t a1[4] = {ld32(&As[r0][2 * t]), ld32(&As[r1][2 * t]), ld32(&As[r0][2 * t + 8]),
+                            ld32(&As[r1][2 * t + 8])};
+    uint32_t h1[4][4];
+#pragma unroll
+    for (int ks = 0; ks < 4; ks++) {
+      float c[2][4];
+#pragma unroll
+      for (int hh = 0; hh < 2; hh++) {
+        const int nt = 2 * ks + hh, col = nt * 8 + 2 * t;
+        c[hh][0] = c[hh][2] = S.b1[col];
+        c[hh][1] = c[hh][3] = S.b1[col + 1];
+        mma_bf16(c[hh], a1, ld32(&S.w1[nt * 8 + g][2 * t]), ld32(&S.w1[nt * 8 + g][2 * t + 8]));
+      }
+      h1[ks][0] = pack2(silu_f(c[0][0]), silu_f(c[0][1]));
+      h1[ks][1] = pack2(silu_f(c[0][2]), silu_f(c[0][3]));
+      h1[ks][2] = pack2(silu_f(c[1][0]), silu_f(c[1][1]));
+      h1[ks][3] = pack2(silu_f(c[1][2]), silu_f(c[1][3]));
+    }
+    uint32_t h2[4][4];
+#pragma unroll
+    for (int ks2 = 0; ks2 < 4; ks2++) {
+      float c[2][4];
+#pragma unroll
+      for (int hh = 0; hh < 2; hh++) {
+        const int nt = 2 * ks2 + hh, col = nt * 8 + 2 * t;
+        c[hh][0] = c[hh][2] = S.b2[col];
+        c[hh][1] = c[hh][3] = S.b2[col + 1];
+#pragma unroll
+        for (int ks = 0; ks < 4; ks++)
+          mma_bf16(c[hh], h1[ks], ld32(&S.w2[nt * 8 + g][16 * ks + 2 * t]),
+                   ld32(&S.w2[nt * 8 + g][16 * ks + 2 * t + 8]));
+      }
+      h2[ks2][0] = pack2(silu_f(c[0][0]), silu_f(c[0][1]));
+      h2[ks2][1] = pack2(silu_f(c[0][2]), silu_f(c[0][3]));
+      h2[ks2][2] = pack2(silu_f(c[1][0]), silu_f(c[1][1]));
+      h2[ks2][3] = pack2(silu_f(c[1][2]), silu_f(c[1][3]));
+    }
+    float c3[4] = {S.b3[2 * t], S.b3[2 * t + 1], S.b3[2 * t], S.b3[2 * t + 1]};
+#pragma unroll
+    for (int ks = 0; ks < 4; ks++)
+      mma_bf16(c3, h2[ks], ld32(&S.w3[g][16 * ks + 2 * t]), ld32(&S.w3[g][16 * ks + 2 * t + 8]));
+    if (t < 2) {
+      Out[r0][2 * t] = c3[0];
+      Out[r0][2 * t + 1] = c3[1];
+      Out[r1][2 * t] = c3[2];
+      Out[r1][2 * t + 1] = c3[3];
+    }
+  }
+  __syncwarp();
+#pragma unroll
+  for (int k = 0; k < kOut; k++) o[k] = Out[lane][k];
+  __syncwarp();
+}
+
+struct Head {
+  Vec3 mu;
+  float kappa;
+};
+
+__device__ __forceinline__ Head mlp_head(const float (&o)[kOut], float kappa_max) {
+  Head h;
+  const float na = sqrtf(fmaf(o[0], o[0], fmaf(o[1], o[1], o[2] * o[2])));
+  if (na > 1e-12f) {
+    const float inv = 1.f / na;
+    h.mu = Vec3{o[0] * inv, o[1] * inv, o[2] * inv};
+  } else {
+    h.mu = Vec3{0.f, 0.f, 1.f};
+  }
+  const float kr = o[3] > 20.f ? o[3] : log1pf(expf(o[3]));
+  h.kappa = fminf(fmaxf(kr, kKappaMin), kappa_max);
+  return h;
+}
+
+// log(4 pi q(n)) of the mixture at t = mu.n.
+__device__ __forceinline__ float log_q(float t, float kappa) {
+  const float at = fabsf(t);
+  const float g = kappa * (expf(kappa * (at - 1.f)) + expf(-kappa * (at + 1.f))) / (-expm1f(-2.f * kappa));
+  return logf(fmaf(1.f - kEps, g, kEps));
+}
+
+// A draw from the mixture: u_mix < 0.05 uniform on the sphere, else the vMF about mu by Wood's method with a
+// random sign.
+__device__ __forceinline__ Vec3 sample_proposal(const Head &h, float u_mix, float u_w, float u_phi, bool neg) {
+  const bool uni = u_mix < kEps;
+  float w;
+  Vec3 base;
+  if (uni) {
+    w = fmaf(2.f, u_w, -1.f);
+    base = Vec3{0.f, 0.f, 1.f};
+  } else {
+    w = 1.f + log1pf((1.f - u_w) * expm1f(-2.f * h.kappa)) / h.kappa;
+    w = fminf(fmaxf(w, -1.f), 1.f);
+    base = h.mu;
+  }
+  // orthonormal e1, e2 perpendicular to base: e1 = base x (x or y axis), e2 = base x e1
+  Vec3 e1 = fabsf(base.x) < 0.9f ? Vec3{0.f, base.z, -base.y} : Vec3{-base.z, 0.f, base.x};
+  const float i1 = rsqrtf(dot(e1, e1));
+  e1 = Vec3{e1.x * i1, e1.y * i1, e1.z * i1};
+  const Vec3 e2{base.y * e1.z - base.z * e1.y, base.z * e1.x - base.x * e1.z, base.x * e1.y - base.y * e1.x};
+  const float r = sqrtf(fmaxf(0.f, 1.f - w * w));
+  float sp, cp;
+  sincospif(2.f * u_phi, &sp, &cp);
+  Vec3 v{fmaf(w, base.x, r * fmaf(cp, e1.x, sp * e2.x)), fmaf(w, base.y, r * fmaf(cp, e1.y, sp * e2.y)),
+         fmaf(w, base.z, r * fmaf(cp, e1.z, sp * e2.z))};
+  const float inv = rsqrtf(dot(v, v));
+  const float sgn = (neg && !uni) ? -inv : inv;
+  return Vec3{v.x * sgn, v.y * sgn, v.z * sgn};
+}
+
+__device__ __forceinline__ float u24(uint32_t v) { return (float)(v >> 8) * 0x1p-24f; }
+
+// ---- the learned sweep: one colour, one thread per site ----------------------------------------------------------
+template <int POT, int GEO>
+__global__ void __launch_bounds__(kThreads) k_sweep_learned(ModelDev m, const RepDesc *__restrict__ reps,
+                                                            RepState *__restrict__ st, float *__restrict__ dir,
+                                                            const uint8_t *__restrict__ pt,
+                                                            const float *__restrict__ nrm,
+                                                            const unsigned long long *__restrict__ sweep_ctr,
+                                                            int colour, const int *__restrict__ blk_rep,
+                                                            const long long *__restrict__ blk_base, int n_blocks,
+                                                            const MlpDev *__restrict__ mlp, float kappa_max) {
+  __shared__ __align__(16) MlpDev S;
+  __shared__ __align__(16) __nv_bfloat16 As[kThreads / 32][32][24];
+  __shared__ float Out[kThreads / 32][32][4];
+  for (int i = threadIdx.x; i < (int)(sizeof(MlpDev) / 16); i += blockDim.x)
+    reinterpret_cast<uint4 *>(&S)[i] = reinterpret_cast<const uint4 *>(mlp)[i];
+  __syncthreads();
+  const int warp = threadIdx.x >> 5;
+  const unsigned long long sweep = *sweep_ctr;
+  for (int b = blockIdx.x; b < n_blocks; b += gridDim.x) {
+    const int rep = blk_rep[b];
+    const RepDesc R = reps[rep];
+    const RepState St = st[rep];
+    const long long q = blk_base[b] + threadIdx.x;
+    const int hx = (R.nx + 1) >> 1;
+    const long long total = (long long)hx * R.ny * R.nz;
+    bool valid = false;
+    int x = 0, y = 0, z = 0, sid = -1;
+    Vec3 n{0.f, 0.f, 1.f}, s{0.f, 0.f, 0.f};
+    Vec3 nb[6];
+    float w[6];
+#pragma unroll
+    for (int d = 0; d < 6; d++) {
+      nb[d] = Vec3{0.f, 0.f, 0.f};
+      w[d] = 0.f;
+    }
+    if (q < total) {
+      const int xh = (int)(q % hx);
+      const long long row = q / hx;
+      y = (int)(row % R.ny);
+      z = (int)(row / R.ny);
+      x = 2 * xh + ((colour + y + z) & 1);
+      if (x < R.nx) valid = gather_site_w<GEO>(R, dir, pt, nrm, x, y, z, n, nb, w, sid, s);
+    }
+    float f[kIn] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (valid) site_features(nb, w, St.T, f);
+    float o[kOut];
+    warp_mlp(S, As[warp], Out[warp], f, o);
+    unsigned accepted = 0;
+    if (valid) {
+      const Head h = mlp_head(o, kappa_max);
+      const U4 u = site_draws(R.seed, sweep, (uint32_t)site_linear(R, x, y, z), 1);
+      const Vec3 nn = sample_proposal(h, u24(u.x), u24(u.y), u24(u.z), (u.x & 1u) != 0u);
+      float b_old, b_new;
+      bond_sum2<POT, false, true, float>(m, n, nn, nb, w, b_old, b_new);
+      const float e_old = __fadd_rn(b_old, single_energy<true>(m, n, sid, s, St.elecE));
+      const float e_new = __fadd_rn(b_new, single_energy<true>(m, nn, sid, s, St.elecE));
+      const float dE = __fadd_rn(e_new, -e_old);
+      bool acc;
+      if (St.T > 0.f) {
+        const float lr = log_q(dot(h.mu, n), h.kappa) - log_q(dot(h.mu, nn), h.kappa);
+        acc = u24(u.w) < expf(fmaf(-dE, 1.f / St.T, lr));
+      } else {
+        acc = dE <= 0.f;
+      }
+      if (acc) {
+        dir[dir_index(R, 0, x, y, z)] = nn.x;
+        dir[dir_index(R, 1, x, y, z)] = nn.y;
+        dir[dir_index(R, 2, x, y, z)] = nn.z;
+        accepted = 1;
+      }
+    }
+    const unsigned wsum = __reduce_add_sync(0xffffffffu, accepted);
+    if ((threadIdx.x & 31) == 0 && wsum) atomicAdd(&st[rep].acc, (unsigned long long)wsum);
+  }
+}
+
+// Network outputs (before the head) for feature rows, for parity tests of the tensor-core path.
+__global__ void __launch_bounds__(kThreads) k_mlp_forward(const MlpDev *__restrict__ mlp,
+                                                          const float *__restrict__ feat, long long n,
+                                                          float *__restrict__ out) {
+  __shared__ __align__(16) MlpDev S;
+  __shared__ __align__(16) __nv_bfloat16 As[kThreads / 32][32][24];
+  __shared__ float Out[kThreads / 32][32][4];
+  for (int i = threadIdx.x; i < (int)(sizeof(MlpDev) / 16); i += blockDim.x)
+    reinterpret_cast<uint4 *>(&S)[i] = reinterpret_cast<const uint4 *>(mlp)[i];
+  __syncthreads();
+  const int warp = threadIdx.x >> 5;
+  for (long long base = (long long)blockIdx.x * kThreads; base < n; base += (long long)gridDim.x * kThreads) {
+    const long long i = base + threadIdx.x;
+    float f[kIn];
+#pragma unroll
+    for (int k = 0; k < kIn; k++) f[k] = i < n ? feat[i * kFeat + k] : 0.f;
+    float o[kOut];
+    warp_mlp(S, As[warp], Out[warp], f, o);
+    if (i < n)
+#pragma unroll
+      for (int k = 0; k < kOut; k++) out[i * kOut + k] = o[k];
+  }
+}
+
+// Training samples: n sites of one replica drawn with Philox(seed, sample index), their features and directors.
+template <int GEO>
+__global__ void k_extract_samples(const RepDesc *__restrict__ reps, const RepState *__restrict__ st,
+                                  const float *__restrict__ dir, const uint8_t *__restrict__ pt,
+                                  const float *__restrict__ nrm, int rep, long long n, unsigned long long seed,
+                                  float *__restrict__ feat, float *__restrict__ dirs) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const RepDesc R = reps[rep];
+  const U4 u = philox4x32_10((uint32_t)i, (uint32_t)(i >> 32), 0u, 3u, (uint32_t)seed, (uint32_t)(seed >> 32));
+  const unsigned long long N = (unsigned long long)R.nx * R.ny * R.nz;
+  const unsigned long long site = (((unsigned long long)u.x << 32) | u.y) % N;
+  const int x = (int)(site % R.nx);
+  const unsigned long long row = site / R.nx;
+  const int y = (int)(row % R.ny), z = (int)(row / R.ny);
+  Vec3 nv, nb[6], s;
+  float w[6];
+  int sid;
+  float f[kIn] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  const bool valid = gather_site_w<GEO>(R, dir, pt, nrm, x, y, z, nv, nb, w, sid, s);
+  if (valid) site_features(nb, w, st[rep].T, f);
+#pragma unroll
+  for (int k = 0; k < kIn; k++) feat[i * kFeat + k] = f[k];
+  feat[i * kFeat + 7] = valid ? 1.f : 0.f;
+  dirs[i * 3 + 0] = valid ? nv.x : 0.f;
+  dirs[i * 3 + 1] = valid ? nv.y : 0.f;
+  dirs[i * 3 + 2] = valid ? nv.z : 0.f;
+}
+
+// ---- training ------------------------------------------------------------------------------------------------
+constexpr int kTB = 64;            // samples (threads) per training block
+constexpr int kHP = kH + 1;        // row pitch of the per-sample activation arrays
+constexpr int kWPad = kNP + 4;     // BF16-rounded weights in shared memory
+constexpr size_t kTrainSmem = sizeof(float) * (kWPad + kTB * 9 + 4 * kTB * kHP + kTB * 5 + kTB);
+
+// Forward and backward pass of kTB samples (one per thread) with the pass copy wr of the parameters; writes this block's
+// parameter gradient of the mean loss (scale = 1 / batch) and its loss sum to partial[blockIdx.x][0 .. kNP].
+__global__ void __launch_bounds__(kTB) k_mlp_grad(const float *__restrict__ wr, const float *__restrict__ feat,
+                                                  const float *__restrict__ dirs, long long n, float kappa_max,
+                                                  float scale, float *__restrict__ partial) {
+  extern __shared__ float sm[];
+  float *W = sm;
+  float *X = W + kWPad;            // [kTB][9]
+  float *H1 = X + kTB * 9;         // [kTB][kHP]
+  float *H2 = H1 + kTB * kHP;
+  float *DZ1 = H2 + kTB * kHP;
+  float *DZ2 = DZ1 + kTB * kHP;
+  float *DO = DZ2 + kTB * kHP;     // [kTB][5]
+  float *LS = DO + kTB * 5;        // [kTB]
+  const int tid = threadIdx.x;
+  for (int i = tid; i < kNP; i += kTB) W[i] = wr[i];
+  __syncthreads();
+  const long long s = (long long)blockIdx.x * kTB + tid;
+  const bool valid = s < n && feat[s * kFeat + 7] != 0.f;
+  float x[kIn];
+#pragma unroll
+  for (int k = 0; k < kIn; k++) {
+    x[k] = valid ? bf16r(feat[s * kFeat + k]) : 0.f;
+    X[tid * 9 + k] = x[k];
+  }
+  float z1[kH], h1[kH];
+#pragma unroll 8
+  for (int j = 0; j < kH; j++) {
+    float a = W[oB1 + j];
+#pragma unroll
+    for (int k = 0; k < kIn; k++) a = fmaf(W[oW1 + j * kIn + k], x[k], a);
+    z1[j] = a;
+    h1[j] = bf16r(silu_f(a));
+    H1[tid * kHP + j] = h1[j];
+  }
+  float z2[kH], h2[kH];
+#pragma unroll 4
+  for (int j = 0; j < kH; j++) {
+    float a = W[oB2 + j];
+#pragma unroll
+    for (int i = 0; i < kH; i++) a = fmaf(W[oW2 + j * kH + i], h1[i], a);
+    z2[j] = a;
+    h2[j] = bf16r(silu_f(a));
+    H2[tid * kHP + j] = h2[j];
+  }
+  float o[kOut];
+#pragma unroll
+  for (int mo = 0; mo < kOut; mo++) {
+    float a = W[oB3 + mo];
+#pragma unroll
+    for (int j = 0; j < kH; j++) a = fmaf(W[oW3 + mo * kH + j], h2[j], a);
+    o[mo] = a;
+  }
+  // head, loss and d loss / d o
+  float dout[kOut] = {0.f, 0.f, 0.f, 0.f};
+  float loss = 0.f;
+  if (valid) {
+    const float nx = dirs[s * 3], ny = dirs[s * 3 + 1], nz = dirs[s * 3 + 2];
+    const float na = sqrtf(fmaf(o[0], o[0], fmaf(o[1], o[1], o[2] * o[2])));
+    const float inv = 1.f / fmaxf(na, 1e-20f);
+    const float mx = o[0] * inv, my = o[1] * inv, mz = o[2] * inv;
+    const float kr = o[3] > 20.f ? o[3] : log1pf(expf(o[3]));
+    const float kappa = fminf(fmaxf(kr, kKappaMin), kappa_max);
+    const float t = fmaf(mx, nx, fmaf(my, ny, mz * nz));
+    const float at = fabsf(t);
+    const float g = kappa * (expf(kappa * (at - 1.f)) + expf(-kappa * (at + 1.f))) / (-expm1f(-2.f * kappa));
+    const float den = fmaf(1.f - kEps, g, kEps);
+    loss = -logf(den);
+    const float th = tanhf(kappa * t);
+    const float dt = -(1.f - kEps) * g * kappa * th / den;
+    const float ikc = kappa < 0.1f ? kappa * (-1.f / 3.f + kappa * kappa / 45.f) : 1.f / kappa - 1.f / tanhf(kappa);
+    float dk = -(1.f - kEps) * g * (ikc + t * th) / den;
+    if (!(kr > kKappaMin && kr < kappa_max)) dk = 0.f;
+    dout[0] = scale * dt * (nx - t * mx) * inv;
+    dout[1] = scale * dt * (ny - t * my) * inv;
+    dout[2] = scale * dt * (nz - t * mz) * inv;
+    dout[3] = scale * dk * sigm_f(o[3]);
+  }
+  LS[tid] = loss;
+#pragma unroll
+  for (int mo = 0; mo < kOut; mo++) DO[tid * 5 + mo] = dout[mo];
+  // backward to the hidden layers (z2 is overwritten with dz2)
+#pragma unroll 4
+  for (int j = 0; j < kH; j++) {
+    float a = 0.f;
+#pragma unroll
+    for (int mo = 0; mo < kOut; mo++) a = fmaf(W[oW3 + mo * kH + j], dout[mo], a);
+    const float sg = sigm_f(z2[j]);
+    z2[j] = a * sg * fmaf(z2[j], 1.f - sg, 1.f);
+    DZ2[tid * kHP + j] = z2[j];
+  }
+#pragma unroll 4
+  for (int i = 0; i < kH; i++) {
+    float a = 0.f;
+#pragma unroll
+    for (int j = 0; j < kH; j++) a = fmaf(W[oW2 + j * kH + i], z2[j], a);
+    const float sg = sigm_f(z1[i]);
+    DZ1[tid * kHP + i] = a * sg * fmaf(z1[i], 1.f - sg, 1.f);
+  }
+  __syncthreads();
+  // this block's weight gradients: thread tid owns column tid of every [out][in] matrix it can
+  float *P = partial + (size_t)blockIdx.x * (kNP + 1);
+  for (int r = 0; r < kH; r++) {  // w2[r][tid] = sum_s dz2[s][r] h1[s][tid]
+    float a = 0.f;
+    for (int q = 0; q < kTB; q++) a = fmaf(DZ2[q * kHP + r], H1[q * kHP + tid], a);
+    P[oW2 + r * kH + tid] = a;
+  }
+  {
+    float a[kIn] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, b1 = 0.f, b2 = 0.f;
+    for (int q = 0; q < kTB; q++) {
+      const float d1 = DZ1[q * kHP + tid];
+#pragma unroll
+      for (int k = 0; k < kIn; k++) a[k] = fmaf(d1, X[q * 9 + k], a[k]);
+      b1 += d1;
+      b2 += DZ2[q * kHP + tid];
+    }
+#pragma unroll
+    for (int k = 0; k < kIn; k++) P[oW1 + tid * kIn + k] = a[k];
+    P[oB1 + tid] = b1;
+    P[oB2 + tid] = b2;
+  }
+#pragma unroll
+  for (int mo = 0; mo < kOut; mo++) {  // w3[mo][tid]
+    float a = 0.f;
+    for (int q = 0; q < kTB; q++) a = fmaf(DO[q * 5 + mo], H2[q * kHP + tid], a);
+    P[oW3 + mo * kH + tid] = a;
+  }
+  if (tid < kOut) {
+    float a = 0.f;
+    for (int q = 0; q < kTB; q++) a += DO[q * 5 + tid];
+    P[oB3 + tid] = a;
+  }
+  if (tid == 0) {
+    float a = 0.f;
+    for (int q = 0; q < kTB; q++) a += LS[q];
+    P[kNP] = a;
+  }
+}
+
+// Fixed-order FP64 sum of the block partials: gradient (and loss sum in out[kNP]).
+__global__ void k_grad_reduce(const float *__restrict__ partial, int nb, double *__restrict__ out) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p > kNP) return;
+  double a = 0.0;
+  for (int b = 0; b < nb; b++) a += (double)partial[(size_t)b * (kNP + 1) + p];
+  out[p] = a;
+}
+
+// Biases stay FP32 in every pass (as in inference); weights are rounded to BF16.
+__device__ __forceinline__ float pass_value(int p, float v) {
+  const bool bias = (p >= oB1 && p < oB1 + kH) || (p >= oB2 && p < oB2 + kH) || p >= oB3;
+  return bias ? v : bf16r(v);
+}
+
+// Adam on the FP32 master parameters, then their copy for the next forward pass (weights BF16-rounded).
+__global__ void k_adam(const double *__restrict__ grad, float *__restrict__ params, float *__restrict__ wr,
+                       float *__restrict__ m1, float *__restrict__ m2, float lr, float bc1, float bc2) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= kNP) return;
+  const float g = (float)grad[p];
+  const float a = fmaf(0.9f, m1[p], 0.1f * g), b = fmaf(0.999f, m2[p], 0.001f * g * g);
+  m1[p] = a;
+  m2[p] = b;
+  const float v = params[p] - lr * (a / bc1) / (sqrtf(b / bc2) + 1e-8f);
+  params[p] = v;
+  wr[p] = pass_value(p, v);
+}
+
+__global__ void k_round(const float *__restrict__ params, float *__restrict__ wr) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < kNP) wr[p] = pass_value(p, params[p]);
+}
+
+// ---- launchers -------------------------------------------------------------------------------------------------
+template <int POT>
+static void sweep_learned_pot(const LaunchCtx &c, int geo, const BlockTable &t, int colour, const MlpDev *mlp,
+                              float kappa_max, int grid) {
+  switch (geo) {
+    case GEO_BULK:
+      k_sweep_learned<POT, GEO_BULK><<<grid, kThreads, 0, c.stream>>>(c.model, c.reps, c.state, c.dir, c.pt, c.nrm,
+                                                                       c.sweep_ctr, colour, t.rep, t.base, t.n_blocks,
+                                                                       mlp, kappa_max);
+      break;
+    case GEO_SLAB:
+      k_sweep_learned<POT, GEO_SLAB><<<grid, kThreads, 0, c.stream>>>(c.model, c.reps, c.state, c.dir, c.pt, c.nrm,
+                                                                       c.sweep_ctr, colour, t.rep, t.base, t.n_blocks,
+                                                                       mlp, kappa_max);
+      break;
+    default:
+      k_sweep_learned<POT, GEO_PT><<<grid, kThreads, 0, c.stream>>>(c.model, c.reps, c.state, c.dir, c.pt, c.nrm,
+                                                                     c.sweep_ctr, colour, t.rep, t.base, t.n_blocks,
+                                                                     mlp, kappa_max);
+  }
+}
+
+cudaError_t launch_sweep_learned(const LaunchCtx &c, int geo, const BlockTable &half, const MlpDev *mlp,
+                                 float kappa_max) {
+  if (half.n_blocks == 0) return cudaSuccess;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = std::min(half.n_blocks, sms * 8);
+  for (int colour = 0; colour < 2; colour++) {
+    if (c.model.potential == POT_GHRL)
+      sweep_learned_pot<POT_GHRL>(c, geo, half, colour, mlp, kappa_max, grid);
+    else if (c.model.potential == POT_PEAR)
+      sweep_learned_pot<POT_PEAR>(c, geo, half, colour, mlp, kappa_max, grid);
+    else
+      sweep_learned_pot<POT_LL>(c, geo, half, colour, mlp, kappa_max, grid);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace mcl
+
+// ---- C ABI -----------------------------------------------------------------------------------------------------
+using namespace mcl;
+
+#define CKL(call)                                        \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);  \
+  } while (0)
+
+struct mcl_trainer {
+  long long max_batch = 0;
+  int max_blocks = 0;
+  float kappa_max = 500.f;
+  float *d_params = nullptr, *d_wr = nullptr, *d_m1 = nullptr, *d_m2 = nullptr, *d_partial = nullptr;
+  double *d_grad = nullptr;
+  long long steps = 0;
+  cudaStream_t stream = nullptr;
+};
+
+static bool finite_params(const mcl_mlp *p) {
+  const float *f = reinterpret_cast<const float *>(p);
+  for (int i = 0; i < kNP; i++)
+    if (!std::isfinite(f[i])) return false;
+  return true;
+}
+
+extern "C" {
+
+int mcl_set_proposal(mcl_engine *e, const mcl_mlp *mlp, float kappa_max) {
+  if (!e) return fail(MCL_ERR_ARG, "null engine");
+  CKL(cudaStreamSynchronize(e->stream));
+  if (!mlp) {
+    if (e->d_mlp) cudaFree(e->d_mlp);
+    e->d_mlp = nullptr;
+    return MCL_OK;
+  }
+  if (!(kappa_max > kKappaMin && kappa_max <= 1e4f))
+    return fail(MCL_ERR_ARG, "mcl_set_proposal: kappa_max must lie in (1e-3, 1e4]");
+  if (!finite_params(mlp)) return fail(MCL_ERR_NONFINITE, "mcl_set_proposal: non-finite weight");
+  MlpDev h;
+  to_device_layout(*mlp, h);
+  if (!e->d_mlp) CKL(cudaMalloc(&e->d_mlp, sizeof(MlpDev)));
+  CKL(cudaMemcpy(e->d_mlp, &h, sizeof h, cudaMemcpyHostToDevice));
+  e->kappa_max = kappa_max;
+  return MCL_OK;
+}
+
+int mcl_set_adaptation(mcl_engine *e, int enable) {
+  if (!e) return fail(MCL_ERR_ARG, "null engine");
+  e->adapt = enable != 0;
+  return MCL_OK;
+}
+
+int mcl_extract_samples(mcl_engine *e, int replica, long long n, unsigned long long seed, float *d_features,
+                        float *d_directors) {
+  if (!e) return fail(MCL_ERR_ARG, "null engine");
+  if (replica < 0 || replica >= e->n_rep) return fail(MCL_ERR_ARG, "replica %d outside 0..%d", replica, e->n_rep - 1);
+  if (n < 0 || (n > 0 && (!d_features || !d_directors))) return fail(MCL_ERR_ARG, "mcl_extract_samples: bad buffers");
+  if (!e->geometry_set) return fail(MCL_ERR_STATE, "custom geometry: call mcl_set_geometry first");
+  if (n == 0) return MCL_OK;
+  const LaunchCtx c = e->ctx();
+  const int threads = 256;
+  const long long blocks = (n + threads - 1) / threads;
+  if (blocks > 0x7FFFFFFFll) return fail(MCL_ERR_ARG, "mcl_extract_samples: too many samples");
+  switch (e->geo) {
+    case GEO_BULK:
+      k_extract_samples<GEO_BULK><<<(unsigned)blocks, threads, 0, c.stream>>>(c.reps, c.state, c.dir, c.pt, c.nrm,
+                                                                              replica, n, seed, d_features, d_directors);
+      break;
+    case GEO_SLAB:
+      k_extract_samples<GEO_SLAB><<<(unsigned)blocks, threads, 0, c.stream>>>(c.reps, c.state, c.dir, c.pt, c.nrm,
+                                                                              replica, n, seed, d_features, d_directors);
+      break;
+    default:
+      k_extract_samples<GEO_PT><<<(unsigned)blocks, threads, 0, c.stream>>>(c.reps, c.state, c.dir, c.pt, c.nrm,
+                                                                            replica, n, seed, d_features, d_directors);
+  }
+  CKL(cudaGetLastError());
+  e->launches++;
+  CKL(cudaStreamSynchronize(c.stream));
+  return MCL_OK;
+}
+
+int mcl_mlp_forward(const mcl_mlp *mlp, const float *d_features, long long n, float *d_out, void *stream) {
+  if (!mlp || n < 0 || (n > 0 && (!d_features || !d_out))) return fail(MCL_ERR_ARG, "mcl_mlp_forward: bad arguments");
+  if (n == 0) return MCL_OK;
+  MlpDev h;
+  to_device_layout(*mlp, h);
+  MlpDev *d = nullptr;
+  CKL(cudaMalloc(&d, sizeof h));
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t err = cudaMemcpyAsync(d, &h, sizeof h, cudaMemcpyHostToDevice, st);
+  if (err == cudaSuccess) {
+    const long long blocks = std::min<long long>((n + kThreads - 1) / kThreads, 148ll * 16);
+    k_mlp_forward<<<(unsigned)blocks, kThreads, 0, st>>>(d, d_features, n, d_out);
+    err = cudaGetLastError();
+  }
+  if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+  cudaFree(d);
+  if (err != cudaSuccess) return cuda_fail(err, "mcl_mlp_forward");
+  return MCL_OK;
+}
+
+int mcl_trainer_create(const mcl_mlp *init, long long max_batch, float kappa_max, mcl_trainer **out) {
+  if (!init || !out || max_batch < 1) return fail(MCL_ERR_ARG, "mcl_trainer_create: bad arguments");
+  *out = nullptr;
+  if (!(kappa_max > kKappaMin && kappa_max <= 1e4f)) return fail(MCL_ERR_ARG, "mcl_trainer_create: bad kappa_max");
+  if (!finite_params(init)) return fail(MCL_ERR_NONFINITE, "mcl_trainer_create: non-finite weight");
+  const long long nb = (max_batch + kTB - 1) / kTB;
+  if (nb > (1 << 24)) return fail(MCL_ERR_ARG, "mcl_trainer_create: max_batch too large");
+  mcl_trainer *t = new mcl_trainer();
+  t->max_batch = max_batch;
+  t->max_blocks = (int)nb;
+  t->kappa_max = kappa_max;
+  auto bad = [&](cudaError_t err, const char *what) {
+    mcl_trainer_destroy(t);
+    return cuda_fail(err, what);
+  };
+  cudaError_t err;
+  if ((err = cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking)) != cudaSuccess) return bad(err, "stream");
+  if ((err = cudaMalloc(&t->d_params, kNP * sizeof(float))) != cudaSuccess) return bad(err, "cudaMalloc");
+  if ((err = cudaMalloc(&t->d_wr, kNP * sizeof(float))) != cudaSuccess) return bad(err, "cudaMalloc");
+  if ((err = cudaMalloc(&t->d_m1, kNP * sizeof(float))) != cudaSuccess) return bad(err, "cudaMalloc");
+  if ((err = cudaMalloc(&t->d_m2, kNP * sizeof(float))) != cudaSuccess) return bad(err, "cudaMalloc");
+  if ((err = cudaMalloc(&t->d_grad, (kNP + 1) * sizeof(double))) != cudaSuccess) return bad(err, "cudaMalloc");
+  if ((err = cudaMalloc(&t->d_partial, (size_t)nb * (kNP + 1) * sizeof(float))) != cudaSuccess)
+    return bad(err, "cudaMalloc");
+  if ((err = cudaMemcpy(t->d_params, init, kNP * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess)
+    return bad(err, "cudaMemcpy");
+  if ((err = cudaMemset(t->d_m1, 0, kNP * sizeof(float))) != cudaSuccess) return bad(err, "cudaMemset");
+  if ((err = cudaMemset(t->d_m2, 0, kNP * sizeof(float))) != cudaSuccess) return bad(err, "cudaMemset");
+  k_round<<<(kNP + 255) / 256, 256, 0, t->stream>>>(t->d_params, t->d_wr);
+  if ((err = cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrainSmem)) !=
+      cudaSuccess)
+    return bad(err, "cudaFuncSetAttribute");
+  if ((err = cudaStreamSynchronize(t->stream)) != cudaSuccess) return bad(err, "k_round");
+  *out = t;
+  return MCL_OK;
+}
+
+static int trainer_grad(mcl_trainer *t, const float *d_features, const float *d_directors, long long n) {
+  if (!t || !d_features || !d_directors || n < 1) return fail(MCL_ERR_ARG, "trainer: bad arguments");
+  if (n > t->max_batch) return fail(MCL_ERR_ARG, "trainer: batch %lld exceeds max_batch %lld", n, t->max_batch);
+  const int nb = (int)((n + kTB - 1) / kTB);
+  k_mlp_grad<<<nb, kTB, kTrainSmem, t->stream>>>(t->d_wr, d_features, d_directors, n, t->kappa_max, 1.f / (float)n,
+                                                t->d_partial);
+  CKL(cudaGetLastError());
+  k_grad_reduce<<<(kNP + 1 + 255) / 256, 256, 0, t->stream>>>(t->d_partial, nb, t->d_grad);
+  CKL(cudaGetLastError());
+  return MCL_OK;
+}
+
+int mcl_trainer_gradient(mcl_trainer *t, const float *d_features, const float *d_directors, long long n,
+                         mcl_mlp *grad, double *loss) {
+  int rc = trainer_grad(t, d_features, d_directors, n);
+  if (rc) return rc;
+  std::vector<double> g(kNP + 1);
+  CKL(cudaMemcpyAsync(g.data(), t->d_grad, (kNP + 1) * sizeof(double), cudaMemcpyDeviceToHost, t->stream));
+  CKL(cudaStreamSynchronize(t->stream));
+  if (grad) {
+    float *f = reinterpret_cast<float *>(grad);
+    for (int i = 0; i < kNP; i++) f[i] = (float)g[i];
+  }
+  if (loss) *loss = g[kNP] / (double)n;
+  return MCL_OK;
+}
+
+int mcl_trainer_step(mcl_trainer *t, const float *d_features, const float *d_directors, long long n, float lr,
+                     double *loss) {
+  if (!(lr > 0.f && lr < 1.f)) return fail(MCL_ERR_ARG, "mcl_trainer_step: learning rate must lie in (0, 1)");
+  int rc = trainer_grad(t, d_features, d_directors, n);
+  if (rc) return rc;
+  t->steps++;
+  const float bc1 = 1.f - powf(0.9f, (float)t->steps), bc2 = 1.f - powf(0.999f, (float)t->steps);
+  k_adam<<<(kNP + 255) / 256, 256, 0, t->stream>>>(t->d_grad, t->d_params, t->d_wr, t->d_m1, t->d_m2, lr, bc1, bc2);
+  CKL(cudaGetLastError());
+  if (loss) {
+    double l = 0.0;
+    CKL(cudaMemcpyAsync(&l, t->d_grad + kNP, sizeof(double), cudaMemcpyDeviceToHost, t->stream));
+    CKL(cudaStreamSynchronize(t->stream));
+    *loss = l / (double)n;
+  }
+  return MCL_OK;
+}
+
+int mcl_trainer_get(mcl_trainer *t, mcl_mlp *out) {
+  if (!t || !out) return fail(MCL_ERR_ARG, "mcl_trainer_get: null argument");
+  CKL(cudaStreamSynchronize(t->stream));
+  CKL(cudaMemcpy(out, t->d_params, kNP * sizeof(float), cudaMemcpyDeviceToHost));
+  return MCL_OK;
+}
+
+int mcl_trainer_destroy(mcl_trainer *t) {
+  if (!t) return MCL_OK;
+  if (t->stream) cudaStreamSynchronize(t->stream);
+  cudaFree(t->d_params);
+  cudaFree(t->d_wr);
+  cudaFree(t->d_m1);
+  cudaFree(t->d_m2);
+  cudaFree(t->d_grad);
+  cudaFree(t->d_partial);
+  if (t->stream) cudaStreamDestroy(t->stream);
+  delete t;
+  return MCL_OK;
+}
+
+}  // extern "C"

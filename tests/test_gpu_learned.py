@@ -1,0 +1,176 @@
+"""The learned MH proposal on the GPU against the FP64 oracle (oracle/learned.py): the tensor-core MLP forward pass,
+the features of extracted training samples, the training gradient, and that training lowers the loss. Then the
+property that makes the proposal usable at all: learned sweeps leave the Boltzmann distribution unchanged, so
+<E> and <S> agree with the plain sweep's within their statistical errors, for trained and for untrained
+weights."""
+import numpy as np
+import pytest
+
+from helpers import M
+from oracle import learned as L
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def rand_dirs(n, seed, bias=0.0):
+    rng = np.random.default_rng(seed)
+    v = rng.normal(size=(n, 3))
+    v[:, 2] += bias
+    v /= np.linalg.norm(v, axis=1)[:, None]
+    return v.astype(np.float32).reshape(-1)
+
+
+def perturbed_params(seed):
+    rng = np.random.default_rng(seed)
+    p = L.init_params(3)
+    return (p + 0.3 * rng.normal(size=p.size) * np.abs(p).mean()).astype(np.float32)
+
+
+def engine_ll(L_, T, seed, n_rep=1, sweeps=0):
+    reps = [M.Replica(L_, L_, L_, T=T, seed=seed + r) for r in range(n_rep)]
+    e = M.Engine(M.Model("ll"), reps, M.SCHED_CHECKER2)
+    for r in range(n_rep):
+        e.upload(r, rand_dirs(L_ ** 3, seed + 100 * r, bias=1.5))
+    if sweeps:
+        e.sweeps(sweeps)
+    return e
+
+
+def extract(e, r, n, seed):
+    feat = torch.empty((n, 8), dtype=torch.float32, device="cuda")
+    dirs = torch.empty((n, 3), dtype=torch.float32, device="cuda")
+    e.extract_samples(r, n, seed, feat.data_ptr(), dirs.data_ptr())
+    return feat, dirs
+
+
+def test_mlp_forward_matches_oracle():
+    rng = np.random.default_rng(2)
+    n = 5000
+    x = np.zeros((n, 8), np.float32)
+    x[:, :6] = rng.uniform(-0.5, 1.0, (n, 6))
+    x[:, 6] = rng.uniform(0.2, 1.3, n)
+    x[:, 7] = 1
+    p = perturbed_params(4)
+    feat = torch.from_numpy(x).cuda()
+    out = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+    M.mlp_forward(p, feat.data_ptr(), n, out.data_ptr())
+    got = out.cpu().numpy().astype(np.float64)
+    ref, _ = L.forward(p.astype(np.float64), x[:, :7].astype(np.float64))
+    # same BF16 operands; FP32 sums in another order can move a hidden activation across a BF16 rounding step
+    err = np.abs(got - ref)
+    assert err.max() < 3e-2, err.max()
+    assert err.mean() < 2e-3, err.mean()
+
+
+def test_extracted_features_match_oracle():
+    nx = 10
+    e = engine_ll(nx, 0.8, 5)
+    ni = e.download(0).reshape(-1, 3)
+    feat, dirs = extract(e, 0, 3000, 17)
+    f = feat.cpu().numpy()
+    d = dirs.cpu().numpy()
+    assert np.all(f[:, 7] == 1)
+    index = {tuple(v): i for i, v in enumerate(ni)}
+    sites = np.array([index[tuple(v)] for v in d])
+    assert len(np.unique(sites)) > 900  # the draws cover the lattice
+    x, y, z = sites % nx, (sites // nx) % nx, sites // (nx * nx)
+    nbr = []
+    for dx, dy, dz in [(1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1)]:
+        nbr.append(ni[((x + dx) % nx) + nx * (((y + dy) % nx) + nx * ((z + dz) % nx))])
+    ref = L.features(np.stack(nbr, 1), np.ones((len(sites), 6)), 0.8)
+    np.testing.assert_allclose(f[:, :7], ref, rtol=0, atol=2e-6)
+    e.close()
+
+
+def test_gradient_matches_oracle():
+    e = engine_ll(16, 0.6, 7, sweeps=30)
+    n = 1024
+    feat, dirs = extract(e, 0, n, 3)
+    p = perturbed_params(5)
+    # the axis gradient scales as 1 / |o[0:3]|; a clear axis bias keeps every sample well conditioned, so the
+    # one-ulp BF16 differences of hidden activations between the FP32 and FP64 sums stay small in the gradient
+    p[-2] += 3.0
+    t = M.Trainer(p, n)
+    loss, g = t.gradient(feat.data_ptr(), dirs.data_ptr(), n)
+    x = feat.cpu().numpy()[:, :7].astype(np.float64)
+    d = dirs.cpu().numpy().astype(np.float64)
+    o, _ = L.forward(p.astype(np.float64), x)
+    assert np.linalg.norm(o[:, :3], axis=1).min() > 1.0
+    ref_loss, ref_g = L.loss_and_grad(p.astype(np.float64), x, d)
+    assert abs(loss - ref_loss) < 1e-4 * max(1.0, abs(ref_loss)), (loss, ref_loss)
+    scale = np.abs(ref_g).max()
+    assert np.abs(g - ref_g).max() < 5e-3 * scale, (np.abs(g - ref_g).max(), scale)
+    assert np.linalg.norm(g - ref_g) < 1e-2 * np.linalg.norm(ref_g)
+    t.close()
+    e.close()
+
+
+def train_on(e, n_rep, steps, seed=3, batch=4096, lr=3e-3, snapshots=8, per=4096):
+    """Samples from `snapshots` states of every replica (5 sweeps apart), then `steps` Adam steps."""
+    n = snapshots * n_rep * per
+    feat = torch.empty((n, 8), dtype=torch.float32, device="cuda")
+    dirs = torch.empty((n, 3), dtype=torch.float32, device="cuda")
+    k = 0
+    for s in range(snapshots):
+        e.sweeps(5)
+        for r in range(n_rep):
+            e.extract_samples(r, per, seed * 1000 + s * 17 + r, feat[k:].data_ptr(), dirs[k:].data_ptr())
+            k += per
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    t = M.Trainer(L.init_params(seed).astype(np.float32), batch)
+    losses = []
+    for i in range(steps):
+        idx = torch.randint(0, n, (batch,), generator=g).cuda()
+        fb, db = feat[idx].contiguous(), dirs[idx].contiguous()
+        losses.append(t.step(fb.data_ptr(), db.data_ptr(), batch, lr))
+    p = t.params()
+    t.close()
+    return p, losses
+
+
+def test_training_lowers_the_loss():
+    e = engine_ll(16, 0.5, 11, n_rep=2, sweeps=200)
+    p, losses = train_on(e, 2, 300)
+    first, last = np.mean(losses[:10]), np.mean(losses[-20:])
+    # 0 is the loss of the uniform proposal; the local conditional at T = 0.5 is far narrower
+    assert last < first - 0.5 and last < -0.5, (first, last)
+    # and the trained proposal is accepted far more often than the untrained one
+    e.set_proposal(p)
+    e.sweeps(20, measure=True)
+    acc_trained = e.series(0)["acceptance"][-10:].mean()
+    e.set_proposal(L.init_params(3).astype(np.float32))
+    e.clear_series()
+    e.sweeps(20, measure=True)
+    acc_init = e.series(0)["acceptance"][-10:].mean()
+    assert acc_trained > 0.4 and acc_trained > acc_init + 0.1, (acc_trained, acc_init)
+    e.close()
+
+
+def replica_means(e, n_rep, therm, meas):
+    e.sweeps(therm)
+    e.clear_series()
+    e.sweeps(meas, measure=True)
+    E = np.array([e.series(r)["energy"].mean() for r in range(n_rep)])
+    S = np.array([e.series(r)["S"].mean() for r in range(n_rep)])
+    return E, S
+
+
+@pytest.mark.parametrize("trained", [False, True])
+def test_learned_sweep_keeps_the_equilibrium(trained):
+    T, n_rep, nx = 0.7, 8, 12
+    plain = engine_ll(nx, T, 21, n_rep=n_rep)
+    E0, S0 = replica_means(plain, n_rep, 600, 3000)
+    learned = engine_ll(nx, T, 61, n_rep=n_rep)
+    if trained:
+        learned.sweeps(200)
+        p, _ = train_on(learned, n_rep, 200, snapshots=4, per=2048)
+    else:
+        p = perturbed_params(9)
+    learned.set_proposal(p)
+    E1, S1 = replica_means(learned, n_rep, 600, 3000)
+    for a, b in [(E0, E1), (S0, S1)]:
+        se = np.sqrt(a.var(ddof=1) / n_rep + b.var(ddof=1) / n_rep)
+        assert abs(a.mean() - b.mean()) < 4 * se + 1e-4, (a.mean(), b.mean(), se)
+    plain.close()
+    learned.close()
