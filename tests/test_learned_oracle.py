@@ -81,3 +81,18 @@ def test_tau_int_of_ar1():
         tau, w = L.tau_int(x)
         exact = (1 + phi) / (2 * (1 - phi))
         assert abs(tau - exact) < 0.05 * exact + 0.02, (phi, tau, exact, w)
+
+
+def test_fft_tau_int_matches_direct_sums():
+    from mclics_b200 import analysis as A
+    rng = np.random.default_rng(3)
+    for phi in [0.0, 0.7, 0.97]:
+        n = 20000
+        e = rng.normal(size=n)
+        x = np.empty(n)
+        x[0] = e[0]
+        for i in range(1, n):
+            x[i] = phi * x[i - 1] + e[i]
+        t_ref, w_ref = L.tau_int(x)
+        t, w = A.tau_int(x)
+        assert w == w_ref and abs(t - t_ref) < 1e-9 * max(1.0, t_ref), (phi, t, t_ref, w, w_ref)
