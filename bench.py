@@ -311,6 +311,95 @@ def gpu_arm(args, rank, world, local_rank):
                 acc=float(rec["acceptance"]), cfg=cfg)
 
 
+def learned_compare(args):
+    """Learned vs plain proposal on one workload (c4: LL 128^3 at T = 0.3, 0.8, 1.12): the network is trained on
+    the GPU from plain-sweep states (seed 3), then both proposals run the same number of measured sweeps from the
+    same equilibrated start, and the integrated autocorrelation times of E and S (Sokal windowing) give effective
+    samples per device second. The plain arm keeps ang_var fixed at its adapted value (the fixed-amplitude
+    judge)."""
+    import torch
+    import mclics_b200 as M
+    from mclics_b200 import analysis, learned
+
+    model, reps, cfg, _ = workload(args.workload)
+    creps = [M.Replica(**r) for r in reps]
+    sizes = [r["nx"] * r["ny"] * r["nz"] for r in reps]
+    Ts = [r["T"] for r in reps]
+
+    def engine(seed_off):
+        e = M.Engine(model, creps, M.SCHED_CHECKER2)
+        for i, n in enumerate(sizes):  # ordered start: the nematic states equilibrate within the thermalisation
+            e.upload(i, initial_state(n, "z_noise", 1000 + i + seed_off))
+        return e
+
+    t0 = time.perf_counter()
+    tr = engine(0)
+    tr.sweeps(500)
+    snaps = 20
+    per = max(1, args.train_samples // (snaps * len(reps)))
+    feat, dirs = learned.collect(tr, snapshots=snaps, gap=10, per_snapshot=per, seed=3)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    params, losses = learned.train(feat, dirs, epochs=3, batch=8192, seed=3)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    tr.close()
+    n_samples = int(feat.shape[0])
+    del feat, dirs
+
+    stream = torch.cuda.Stream()
+    K = args.ess_sweeps
+    arms = {}
+    for arm in ("plain", "learned"):
+        e = engine(7)
+        e.set_stream(stream.cuda_stream)
+        e.sweeps(1000)
+        if arm == "plain":
+            e.set_adaptation(False)
+        else:
+            e.set_proposal(params)
+            e.sweeps(100)
+        e.clear_series()
+        e.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        e.sweeps(K, measure=True)
+        ev1.record(stream)
+        ev1.synchronize()
+        sec = ev0.elapsed_time(ev1) / 1e3
+        res = {"device_s": sec, "ms_per_sweep": 1e3 * sec / K, "site_updates_per_s": sum(sizes) * K / sec}
+        for i, T in enumerate(Ts):
+            sr = e.series(i)
+            tE, wE = analysis.tau_int(sr["energy"])
+            tS, wS = analysis.tau_int(sr["S"])
+            mE, dE = analysis.mean_and_error(sr["energy"])
+            mS, dS = analysis.mean_and_error(sr["S"])
+            res[str(T)] = {"tau_E": tE, "window_E": wE, "tau_S": tS, "window_S": wS,
+                           "ess_per_s_E": K / (2 * tE) / sec, "ess_per_s_S": K / (2 * tS) / sec,
+                           "E": mE, "E_err": dE, "S": mS, "S_err": dS,
+                           "acceptance": float(sr["acceptance"].mean())}
+        arms[arm] = res
+        e.close()
+    per_T = {}
+    for T in map(str, Ts):
+        p, l = arms["plain"][T], arms["learned"][T]
+        per_T[T] = {"ess_ratio_E": l["ess_per_s_E"] / p["ess_per_s_E"], "ess_ratio_S": l["ess_per_s_S"] / p["ess_per_s_S"],
+                    "z_E": (l["E"] - p["E"]) / float(np.hypot(l["E_err"], p["E_err"])),
+                    "z_S": (l["S"] - p["S"]) / float(np.hypot(l["S_err"], p["S_err"]))}
+    tnis = str(max(Ts))
+    line = {"metric": "ESS/s (tau_int of E and S), learned vs plain proposal, min over E and S at T=%s" % tnis,
+            "value": min(per_T[tnis]["ess_ratio_E"], per_T[tnis]["ess_ratio_S"]), "unit": "ratio",
+            "higher_is_better": True, "n_gpus": 1, "steps": K, "data": "synthetic", "dtype": "f32 / bf16 MLP",
+            "config": dict(cfg, start="(0,0,1) + 0.1 uniform noise, 1000 thermalisation sweeps",
+                           sweeps_per_arm=K, tau_window="Sokal, c = 5"),
+            "training": {"samples": n_samples, "collect_s": t1 - t0, "train_s": t2 - t1, "steps": len(losses),
+                         "loss_first": float(losses[:20].mean()), "loss_last": float(losses[-50:].mean()),
+                         "seed": 3},
+            "per_T": per_T, "plain": arms["plain"], "learned": arms["learned"]}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -318,6 +407,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="mclics_b200", choices=["mclics_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--learned", action="store_true",
+                    help="learned vs plain proposal: train the proposal network, compare ESS/s of E and S")
+    ap.add_argument("--ess-sweeps", type=int, default=10000)
+    ap.add_argument("--train-samples", type=int, default=10_000_000)
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"],
                     help="c2 (default): the headline GHRL 256^3 slab; others: the remaining configurations")
     args = ap.parse_args()
@@ -326,6 +419,10 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.learned:
+        if rank != 0:
+            return 0
+        return learned_compare(args)
     _, _, config, _ = workload(args.workload) if args.impl != "reference" else workload("c2")
     config = dict(config, step="1 sweep + measurement of every lattice", accumulators="f64 (energy, Q, sum n)",
                   parallelism="independent replicas x%d" % max(1, args.gpus))

@@ -513,9 +513,15 @@ int mcl_sweeps(mcl_engine *e, int n, int measure) {
     } else {
       LaunchCtx c = e->ctx();
       if (ev0) CK(cudaEventRecord(ev0, e->stream));
-      if (e->d_mlp) {
-        CK(launch_sweep_learned(c, e->geo, e->half, e->d_mlp, e->kappa_max));
+      if (e->d_mlp) {  // observables fused into the two colour kernels, finalised over the same block table
+        CK(launch_sweep_learned(c, e->geo, e->half, e->d_mlp, e->kappa_max, measure ? 1 : 0, e->d_partials));
         e->launches += 2;
+        if (ev1) CK(cudaEventRecord(ev1, e->stream));
+        CK(launch_finalize(c, e->half, e->d_partials, measure ? 1 : 0, e->d_series, e->d_series_len, e->d_done));
+        e->launches++;
+        e->ghosts_dirty = true;
+        if (measure) e->series_len++;
+        continue;
       } else if (e->schedule == MCL_SCHED_REF8) {
         CK(launch_sweep_ref8(c, e->geo, e->boxes));
         e->launches += 8;

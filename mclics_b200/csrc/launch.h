@@ -42,10 +42,12 @@ cudaError_t launch_finalize(const LaunchCtx &c, const BlockTable &sites, const d
                             ObsRecord *series, int *series_len, unsigned int *done_ctr);
 // Periodic ghost cells (x then y) of every replica.
 cudaError_t launch_refresh_ghosts(const LaunchCtx &c, int max_ny_nz, int max_px_nz);
-// One sweep with the learned proposal (two colours, in place); mlp: weights in device layout (learned.cu).
+// One sweep with the learned proposal (two colours, in place); mlp: weights in device layout (learned.cu). With
+// measure, the observables of the final state go to partials[block of `half`][kPartials] (reduce them with
+// launch_finalize over the same table).
 struct MlpDev;
 cudaError_t launch_sweep_learned(const LaunchCtx &c, int geo, const BlockTable &half, const MlpDev *mlp,
-                                 float kappa_max);
+                                 float kappa_max, int measure, double *partials);
 // AoS (reference layout) <-> padded SoA for one replica.
 cudaError_t launch_unpack(const LaunchCtx &c, int replica, const RepDesc &host_desc, const float *aos);
 cudaError_t launch_pack(const LaunchCtx &c, int replica, const RepDesc &host_desc, float *aos);

@@ -10,8 +10,8 @@
 // Hastings test u < exp(-dE / T) q(n_old) / q(n_new) leaves the Boltzmann distribution invariant for any weights.
 //
 // The MLP runs on the tensor cores: one warp evaluates 32 sites as two 16-row tiles with mma.sync m16n8k16
-// (BF16 operands, FP32 accumulation); the FP32 accumulator fragments of one layer, after bias and SiLU, are packed
-// to BF16 and used directly as the A fragments of the next layer. Weights live in shared memory, rows padded so
+// (BF16 operands, FP32 accumulation); the FP32 accumulator fragments of one layer, after bias and SiLU (computed
+// as h + h tanh(h), h = z / 2, in packed BF16), are used directly as the A fragments of the next layer. Weights live in shared memory, rows padded so
 // that the fragment loads are free of bank conflicts.
 //
 // Training (maximum likelihood of the local conditional distribution, loss -log(4 pi q(n | features)) over sites
@@ -46,8 +46,9 @@ constexpr float kEps = 0.05f, kKappaMin = 1e-3f;
 constexpr int kFeat = 8;  // floats per sample row: 7 features, validity flag
 
 // Weights in the layout of the tensor-core fragments: [n][k] rows (k contiguous), k padded with zeros (layer 1:
-// 7 -> 16), rows padded to 24 / 72 halves so that the 8 rows of a fragment load hit distinct banks; layer 3 has
-// 8 rows (4 used).
+// 7 -> 16), rows padded to 24 / 72 halves (16-byte aligned rows for ldmatrix, the 8 rows of a fragment in distinct
+// banks); layer 3 has 8 rows (4 used). Weights and biases of the two hidden layers are stored times 1/2 (exact in
+// BF16 and FP32), so that their accumulators hold h = z / 2, the argument of the SiLU form h + h tanh(h).
 struct MlpDev {
   __nv_bfloat16 w1[kH][24];
   __nv_bfloat16 w2[kH][72];
@@ -73,10 +74,10 @@ static void to_device_layout(const mcl_mlp &p, MlpDev &d) {
   memset(&d, 0, sizeof d);
   const float *f = reinterpret_cast<const float *>(&p);
   for (int n = 0; n < kH; n++) {
-    for (int k = 0; k < kIn; k++) set_bf16(&d.w1[n][k], f[oW1 + n * kIn + k]);
-    for (int k = 0; k < kH; k++) set_bf16(&d.w2[n][k], f[oW2 + n * kH + k]);
-    d.b1[n] = f[oB1 + n];
-    d.b2[n] = f[oB2 + n];
+    for (int k = 0; k < kIn; k++) set_bf16(&d.w1[n][k], 0.5f * f[oW1 + n * kIn + k]);
+    for (int k = 0; k < kH; k++) set_bf16(&d.w2[n][k], 0.5f * f[oW2 + n * kH + k]);
+    d.b1[n] = 0.5f * f[oB1 + n];
+    d.b2[n] = 0.5f * f[oB2 + n];
   }
   for (int n = 0; n < kOut; n++) {
     for (int k = 0; k < kH; k++) set_bf16(&d.w3[n][k], f[oW3 + n * kH + k]);
@@ -86,7 +87,6 @@ static void to_device_layout(const mcl_mlp &p, MlpDev &d) {
 
 // ---- device helpers ---------------------------------------------------------------------------------------------
 __device__ __forceinline__ float sigm_f(float z) { return __fdividef(1.f, 1.f + __expf(-fmaxf(z, -80.f))); }
-__device__ __forceinline__ float silu_f(float z) { return z * sigm_f(z); }
 __device__ __forceinline__ float bf16r(float v) { return __bfloat162float(__float2bfloat16_rn(v)); }
 
 __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
@@ -94,6 +94,27 @@ __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
   return *reinterpret_cast<const uint32_t *>(&v);
 }
 __device__ __forceinline__ uint32_t ld32(const __nv_bfloat16 *p) { return *reinterpret_cast<const uint32_t *>(p); }
+
+// SiLU of two halved pre-activations h = z / 2 (FP32), returned as packed BF16 (low half: the first):
+// z sigmoid(z) = h + h tanh(h) with h rounded to BF16, i.e. one tanh.approx.bf16x2 and one bf16x2 fma per pair.
+// Inference and training both use exactly this.
+__device__ __forceinline__ uint32_t silu2h(float h0, float h1) {
+  const uint32_t h = pack2(h0, h1);
+  uint32_t t, r;
+  asm("tanh.approx.bf16x2 %0, %1;" : "=r"(t) : "r"(h));
+  asm("fma.rn.bf16x2 %0, %1, %2, %1;" : "=r"(r) : "r"(h), "r"(t));
+  return r;
+}
+__device__ __forceinline__ uint32_t silu2(float z0, float z1) { return silu2h(0.5f * z0, 0.5f * z1); }
+
+// Four 8x8 BF16 matrices from shared memory; lane l gives the address of row l % 8 of matrix l / 8.
+__device__ __forceinline__ void ldsm_x4(const void *row_addr, uint32_t &r0, uint32_t &r1, uint32_t &r2, uint32_t &r3) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];"
+               : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+               : "r"((unsigned)__cvta_generic_to_shared(row_addr)));
+}
+__device__ __forceinline__ float bf_lo(uint32_t v) { return __uint_as_float(v << 16); }
+__device__ __forceinline__ float bf_hi(uint32_t v) { return __uint_as_float(v & 0xFFFF0000u); }
 
 __device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
   asm volatile(
@@ -132,6 +153,9 @@ __device__ __forceinline__ void site_features(const Vec3 (&nb)[6], const float (
 __device__ __forceinline__ void warp_mlp(const MlpDev &S, __nv_bfloat16 (*As)[24], float (*Out)[4],
                                          const float (&f)[kIn], float (&o)[kOut]) {
   const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  // ldmatrix rows: lane l addresses row (l & 7) of matrix (l >> 3); matrices 0, 1 = k halves of n-tile A,
+  // matrices 2, 3 = k halves of n-tile A + 1 (layers 1, 2) or of k-step + 1 (layer 3)
+  const int lr = lane & 7, lm = lane >> 3;
   uint32_t *row = reinterpret_cast<uint32_t *>(As[lane]);
   row[0] = pack2(f[0], f[1]);
   row[1] = pack2(f[2], f[3]);
@@ -146,19 +170,21 @@ __device__ __forceinline__ void warp_mlp(const MlpDev &S, __nv_bfloat16 (*As)[24
                             ld32(&As[r1][2 * t + 8])};
     uint32_t h1[4][4];
 #pragma unroll
-    for (int ks = 0; ks < 4; ks++) {
+    for (int ks = 0; ks < 4; ks++) {  // n-tiles 2 ks, 2 ks + 1 of layer 1 = k-step ks of layer 2
+      uint32_t bq[4];
+      ldsm_x4(&S.w1[(2 * ks + (lm >> 1)) * 8 + lr][8 * (lm & 1)], bq[0], bq[1], bq[2], bq[3]);
       float c[2][4];
 #pragma unroll
       for (int hh = 0; hh < 2; hh++) {
-        const int nt = 2 * ks + hh, col = nt * 8 + 2 * t;
-        c[hh][0] = c[hh][2] = S.b1[col];
-        c[hh][1] = c[hh][3] = S.b1[col + 1];
-        mma_bf16(c[hh], a1, ld32(&S.w1[nt * 8 + g][2 * t]), ld32(&S.w1[nt * 8 + g][2 * t + 8]));
+        const float2 bb = *reinterpret_cast<const float2 *>(&S.b1[(2 * ks + hh) * 8 + 2 * t]);
+        c[hh][0] = c[hh][2] = bb.x;
+        c[hh][1] = c[hh][3] = bb.y;
+        mma_bf16(c[hh], a1, bq[2 * hh], bq[2 * hh + 1]);
       }
-      h1[ks][0] = pack2(silu_f(c[0][0]), silu_f(c[0][1]));
-      h1[ks][1] = pack2(silu_f(c[0][2]), silu_f(c[0][3]));
-      h1[ks][2] = pack2(silu_f(c[1][0]), silu_f(c[1][1]));
-      h1[ks][3] = pack2(silu_f(c[1][2]), silu_f(c[1][3]));
+      h1[ks][0] = silu2h(c[0][0], c[0][1]);
+      h1[ks][1] = silu2h(c[0][2], c[0][3]);
+      h1[ks][2] = silu2h(c[1][0], c[1][1]);
+      h1[ks][3] = silu2h(c[1][2], c[1][3]);
     }
     uint32_t h2[4][4];
 #pragma unroll
@@ -166,33 +192,42 @@ __device__ __forceinline__ void warp_mlp(const MlpDev &S, __nv_bfloat16 (*As)[24
       float c[2][4];
 #pragma unroll
       for (int hh = 0; hh < 2; hh++) {
-        const int nt = 2 * ks2 + hh, col = nt * 8 + 2 * t;
-        c[hh][0] = c[hh][2] = S.b2[col];
-        c[hh][1] = c[hh][3] = S.b2[col + 1];
-#pragma unroll
-        for (int ks = 0; ks < 4; ks++)
-          mma_bf16(c[hh], h1[ks], ld32(&S.w2[nt * 8 + g][16 * ks + 2 * t]),
-                   ld32(&S.w2[nt * 8 + g][16 * ks + 2 * t + 8]));
+        const float2 bb = *reinterpret_cast<const float2 *>(&S.b2[(2 * ks2 + hh) * 8 + 2 * t]);
+        c[hh][0] = c[hh][2] = bb.x;
+        c[hh][1] = c[hh][3] = bb.y;
       }
-      h2[ks2][0] = pack2(silu_f(c[0][0]), silu_f(c[0][1]));
-      h2[ks2][1] = pack2(silu_f(c[0][2]), silu_f(c[0][3]));
-      h2[ks2][2] = pack2(silu_f(c[1][0]), silu_f(c[1][1]));
-      h2[ks2][3] = pack2(silu_f(c[1][2]), silu_f(c[1][3]));
-    }
-    float c3[4] = {S.b3[2 * t], S.b3[2 * t + 1], S.b3[2 * t], S.b3[2 * t + 1]};
 #pragma unroll
-    for (int ks = 0; ks < 4; ks++)
-      mma_bf16(c3, h2[ks], ld32(&S.w3[g][16 * ks + 2 * t]), ld32(&S.w3[g][16 * ks + 2 * t + 8]));
+      for (int ks = 0; ks < 4; ks++) {
+        uint32_t bq[4];
+        ldsm_x4(&S.w2[(2 * ks2 + (lm >> 1)) * 8 + lr][16 * ks + 8 * (lm & 1)], bq[0], bq[1], bq[2], bq[3]);
+        mma_bf16(c[0], h1[ks], bq[0], bq[1]);
+        mma_bf16(c[1], h1[ks], bq[2], bq[3]);
+      }
+      h2[ks2][0] = silu2h(c[0][0], c[0][1]);
+      h2[ks2][1] = silu2h(c[0][2], c[0][3]);
+      h2[ks2][2] = silu2h(c[1][0], c[1][1]);
+      h2[ks2][3] = silu2h(c[1][2], c[1][3]);
+    }
+    const float2 b3 = *reinterpret_cast<const float2 *>(&S.b3[2 * t]);
+    float c3[4] = {b3.x, b3.y, b3.x, b3.y};
+#pragma unroll
+    for (int kp = 0; kp < 2; kp++) {  // k-steps 2 kp, 2 kp + 1
+      uint32_t bq[4];
+      ldsm_x4(&S.w3[lr][16 * (2 * kp + (lm >> 1)) + 8 * (lm & 1)], bq[0], bq[1], bq[2], bq[3]);
+      mma_bf16(c3, h2[2 * kp], bq[0], bq[1]);
+      mma_bf16(c3, h2[2 * kp + 1], bq[2], bq[3]);
+    }
     if (t < 2) {
-      Out[r0][2 * t] = c3[0];
-      Out[r0][2 * t + 1] = c3[1];
-      Out[r1][2 * t] = c3[2];
-      Out[r1][2 * t + 1] = c3[3];
+      *reinterpret_cast<float2 *>(&Out[r0][2 * t]) = make_float2(c3[0], c3[1]);
+      *reinterpret_cast<float2 *>(&Out[r1][2 * t]) = make_float2(c3[2], c3[3]);
     }
   }
   __syncwarp();
-#pragma unroll
-  for (int k = 0; k < kOut; k++) o[k] = Out[lane][k];
+  const float4 ov = *reinterpret_cast<const float4 *>(Out[lane]);
+  o[0] = ov.x;
+  o[1] = ov.y;
+  o[2] = ov.z;
+  o[3] = ov.w;
   __syncwarp();
 }
 
@@ -215,16 +250,19 @@ __device__ __forceinline__ Head mlp_head(const float (&o)[kOut], float kappa_max
   return h;
 }
 
-// log(4 pi q(n)) of the mixture at t = mu.n.
-__device__ __forceinline__ float log_q(float t, float kappa) {
-  const float at = fabsf(t);
-  const float g = kappa * (expf(kappa * (at - 1.f)) + expf(-kappa * (at + 1.f))) / (-expm1f(-2.f * kappa));
-  return logf(fmaf(1.f - kEps, g, kEps));
+// 4 pi q(n) of the mixture at t = mu.n: 0.95 g + 0.05 with g = kappa cosh(kappa t) / sinh(kappa)
+// = kappa (e^{kappa (|t| - 1)} + e^{-kappa (|t| + 1)}) / (1 - e^{-2 kappa}); inv_den = 1 / (1 - e^{-2 kappa}),
+// e2k = e^{-2 kappa}. One exponential: the second term is e2k / the first.
+__device__ __forceinline__ float q4pi(float t, float kappa, float inv_den, float e2k) {
+  const float e1 = __expf(kappa * (fabsf(t) - 1.f));
+  const float e2 = e1 > 1e-30f ? __fdividef(e2k, e1) : 0.f;
+  return fmaf(1.f - kEps, kappa * (e1 + e2) * inv_den, kEps);
 }
 
 // A draw from the mixture: u_mix < 0.05 uniform on the sphere, else the vMF about mu by Wood's method with a
-// random sign.
-__device__ __forceinline__ Vec3 sample_proposal(const Head &h, float u_mix, float u_w, float u_phi, bool neg) {
+// random sign (em1 = expm1(-2 kappa)).
+__device__ __forceinline__ Vec3 sample_proposal(const Head &h, float em1, float u_mix, float u_w, float u_phi,
+                                                bool neg) {
   const bool uni = u_mix < kEps;
   float w;
   Vec3 base;
@@ -232,7 +270,7 @@ __device__ __forceinline__ Vec3 sample_proposal(const Head &h, float u_mix, floa
     w = fmaf(2.f, u_w, -1.f);
     base = Vec3{0.f, 0.f, 1.f};
   } else {
-    w = 1.f + log1pf((1.f - u_w) * expm1f(-2.f * h.kappa)) / h.kappa;
+    w = 1.f + log1pf((1.f - u_w) * em1) / h.kappa;  // em1 = e^{-2 kappa} - 1
     w = fminf(fmaxf(w, -1.f), 1.f);
     base = h.mu;
   }
@@ -255,17 +293,19 @@ __device__ __forceinline__ float u24(uint32_t v) { return (float)(v >> 8) * 0x1p
 
 // ---- the learned sweep: one colour, one thread per site ----------------------------------------------------------
 template <int POT, int GEO>
-__global__ void __launch_bounds__(kThreads) k_sweep_learned(ModelDev m, const RepDesc *__restrict__ reps,
+__global__ void __launch_bounds__(kThreads, 3) k_sweep_learned(ModelDev m, const RepDesc *__restrict__ reps,
                                                             RepState *__restrict__ st, float *__restrict__ dir,
                                                             const uint8_t *__restrict__ pt,
                                                             const float *__restrict__ nrm,
                                                             const unsigned long long *__restrict__ sweep_ctr,
                                                             int colour, const int *__restrict__ blk_rep,
                                                             const long long *__restrict__ blk_base, int n_blocks,
-                                                            const MlpDev *__restrict__ mlp, float kappa_max) {
+                                                            const MlpDev *__restrict__ mlp, float kappa_max,
+                                                            int measure, double *__restrict__ partials) {
   __shared__ __align__(16) MlpDev S;
+  __shared__ double red[kThreads / 32][kPartials];
   __shared__ __align__(16) __nv_bfloat16 As[kThreads / 32][32][24];
-  __shared__ float Out[kThreads / 32][32][4];
+  __shared__ __align__(16) float Out[kThreads / 32][32][4];
   for (int i = threadIdx.x; i < (int)(sizeof(MlpDev) / 16); i += blockDim.x)
     reinterpret_cast<uint4 *>(&S)[i] = reinterpret_cast<const uint4 *>(mlp)[i];
   __syncthreads();
@@ -301,19 +341,23 @@ __global__ void __launch_bounds__(kThreads) k_sweep_learned(ModelDev m, const Re
     float o[kOut];
     warp_mlp(S, As[warp], Out[warp], f, o);
     unsigned accepted = 0;
+    float ob[kPartials] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     if (valid) {
       const Head h = mlp_head(o, kappa_max);
       const U4 u = site_draws(R.seed, sweep, (uint32_t)site_linear(R, x, y, z), 1);
-      const Vec3 nn = sample_proposal(h, u24(u.x), u24(u.y), u24(u.z), (u.x & 1u) != 0u);
+      const float em1 = expm1f(-2.f * h.kappa);
+      const Vec3 nn = sample_proposal(h, em1, u24(u.x), u24(u.y), u24(u.z), (u.x & 1u) != 0u);
       float b_old, b_new;
       bond_sum2<POT, false, true, float>(m, n, nn, nb, w, b_old, b_new);
-      const float e_old = __fadd_rn(b_old, single_energy<true>(m, n, sid, s, St.elecE));
-      const float e_new = __fadd_rn(b_new, single_energy<true>(m, nn, sid, s, St.elecE));
+      const float s_old = single_energy<true>(m, n, sid, s, St.elecE), s_new = single_energy<true>(m, nn, sid, s, St.elecE);
+      const float e_old = __fadd_rn(b_old, s_old);
+      const float e_new = __fadd_rn(b_new, s_new);
       const float dE = __fadd_rn(e_new, -e_old);
       bool acc;
-      if (St.T > 0.f) {
-        const float lr = log_q(dot(h.mu, n), h.kappa) - log_q(dot(h.mu, nn), h.kappa);
-        acc = u24(u.w) < expf(fmaf(-dE, 1.f / St.T, lr));
+      if (St.T > 0.f) {  // u < e^{-dE/T} q(n) / q(n'), without logarithms
+        const float inv_den = -1.f / em1, e2k = 1.f + em1;
+        const float q_old = q4pi(dot(h.mu, n), h.kappa, inv_den, e2k), q_new = q4pi(dot(h.mu, nn), h.kappa, inv_den, e2k);
+        acc = u24(u.w) * q_new < __expf(-dE / St.T) * q_old;
       } else {
         acc = dE <= 0.f;
       }
@@ -323,9 +367,41 @@ __global__ void __launch_bounds__(kThreads) k_sweep_learned(ModelDev m, const Re
         dir[dir_index(R, 2, x, y, z)] = nn.z;
         accepted = 1;
       }
+      if (measure) {  // the site is final: colour 0 adds its single-site terms, colour 1 2 bond + single
+        const Vec3 nf = acc ? nn : n;
+        const float bf = acc ? b_new : b_old, sf = acc ? s_new : s_old;
+        ob[0] = colour == 0 ? sf : __fadd_rn(__fmul_rn(2.f, bf), sf);
+        ob[1] = fmaf(1.5f * nf.x, nf.x, -0.5f);
+        ob[2] = 1.5f * nf.x * nf.y;
+        ob[3] = 1.5f * nf.x * nf.z;
+        ob[4] = fmaf(1.5f * nf.y, nf.y, -0.5f);
+        ob[5] = 1.5f * nf.y * nf.z;
+        ob[6] = fmaf(1.5f * nf.z, nf.z, -0.5f);
+        ob[7] = nf.x;
+        ob[8] = nf.y;
+        ob[9] = nf.z;
+      }
     }
     const unsigned wsum = __reduce_add_sync(0xffffffffu, accepted);
     if ((threadIdx.x & 31) == 0 && wsum) atomicAdd(&st[rep].acc, (unsigned long long)wsum);
+    if (measure) {  // uniform: table entry b is this block's alone, in both colour launches. FP32 per-site terms
+                    // summed in FP32 over a warp (32 sites), then in FP64.
+#pragma unroll
+      for (int k = 0; k < kPartials; k++) {
+        float v = ob[k];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+        if ((threadIdx.x & 31) == 0) red[warp][k] = (double)v;
+      }
+      __syncthreads();
+      if (threadIdx.x < kPartials) {
+        double v = 0.0;
+        for (int w2 = 0; w2 < kThreads / 32; w2++) v += red[w2][threadIdx.x];
+        double *dst = partials + (long long)b * kPartials + threadIdx.x;
+        *dst = colour == 0 ? v : *dst + v;
+      }
+      __syncthreads();
+    }
   }
 }
 
@@ -335,7 +411,7 @@ __global__ void __launch_bounds__(kThreads) k_mlp_forward(const MlpDev *__restri
                                                           float *__restrict__ out) {
   __shared__ __align__(16) MlpDev S;
   __shared__ __align__(16) __nv_bfloat16 As[kThreads / 32][32][24];
-  __shared__ float Out[kThreads / 32][32][4];
+  __shared__ __align__(16) float Out[kThreads / 32][32][4];
   for (int i = threadIdx.x; i < (int)(sizeof(MlpDev) / 16); i += blockDim.x)
     reinterpret_cast<uint4 *>(&S)[i] = reinterpret_cast<const uint4 *>(mlp)[i];
   __syncthreads();
@@ -414,24 +490,38 @@ __global__ void __launch_bounds__(kTB) k_mlp_grad(const float *__restrict__ wr, 
     X[tid * 9 + k] = x[k];
   }
   float z1[kH], h1[kH];
-#pragma unroll 8
-  for (int j = 0; j < kH; j++) {
-    float a = W[oB1 + j];
+#pragma unroll 4
+  for (int j = 0; j < kH; j += 2) {
+    float a0 = W[oB1 + j], a1 = W[oB1 + j + 1];
 #pragma unroll
-    for (int k = 0; k < kIn; k++) a = fmaf(W[oW1 + j * kIn + k], x[k], a);
-    z1[j] = a;
-    h1[j] = bf16r(silu_f(a));
+    for (int k = 0; k < kIn; k++) {
+      a0 = fmaf(W[oW1 + j * kIn + k], x[k], a0);
+      a1 = fmaf(W[oW1 + (j + 1) * kIn + k], x[k], a1);
+    }
+    z1[j] = a0;
+    z1[j + 1] = a1;
+    const uint32_t hv = silu2(a0, a1);
+    h1[j] = bf_lo(hv);
+    h1[j + 1] = bf_hi(hv);
     H1[tid * kHP + j] = h1[j];
+    H1[tid * kHP + j + 1] = h1[j + 1];
   }
   float z2[kH], h2[kH];
-#pragma unroll 4
-  for (int j = 0; j < kH; j++) {
-    float a = W[oB2 + j];
+#pragma unroll 2
+  for (int j = 0; j < kH; j += 2) {
+    float a0 = W[oB2 + j], a1 = W[oB2 + j + 1];
 #pragma unroll
-    for (int i = 0; i < kH; i++) a = fmaf(W[oW2 + j * kH + i], h1[i], a);
-    z2[j] = a;
-    h2[j] = bf16r(silu_f(a));
+    for (int i = 0; i < kH; i++) {
+      a0 = fmaf(W[oW2 + j * kH + i], h1[i], a0);
+      a1 = fmaf(W[oW2 + (j + 1) * kH + i], h1[i], a1);
+    }
+    z2[j] = a0;
+    z2[j + 1] = a1;
+    const uint32_t hv = silu2(a0, a1);
+    h2[j] = bf_lo(hv);
+    h2[j + 1] = bf_hi(hv);
     H2[tid * kHP + j] = h2[j];
+    H2[tid * kHP + j + 1] = h2[j + 1];
   }
   float o[kOut];
 #pragma unroll
@@ -564,27 +654,27 @@ __global__ void k_round(const float *__restrict__ params, float *__restrict__ wr
 // ---- launchers -------------------------------------------------------------------------------------------------
 template <int POT>
 static void sweep_learned_pot(const LaunchCtx &c, int geo, const BlockTable &t, int colour, const MlpDev *mlp,
-                              float kappa_max, int grid) {
+                              float kappa_max, int grid, int measure, double *partials) {
   switch (geo) {
     case GEO_BULK:
       k_sweep_learned<POT, GEO_BULK><<<grid, kThreads, 0, c.stream>>>(c.model, c.reps, c.state, c.dir, c.pt, c.nrm,
                                                                        c.sweep_ctr, colour, t.rep, t.base, t.n_blocks,
-                                                                       mlp, kappa_max);
+                                                                       mlp, kappa_max, measure, partials);
       break;
     case GEO_SLAB:
       k_sweep_learned<POT, GEO_SLAB><<<grid, kThreads, 0, c.stream>>>(c.model, c.reps, c.state, c.dir, c.pt, c.nrm,
                                                                        c.sweep_ctr, colour, t.rep, t.base, t.n_blocks,
-                                                                       mlp, kappa_max);
+                                                                       mlp, kappa_max, measure, partials);
       break;
     default:
       k_sweep_learned<POT, GEO_PT><<<grid, kThreads, 0, c.stream>>>(c.model, c.reps, c.state, c.dir, c.pt, c.nrm,
                                                                      c.sweep_ctr, colour, t.rep, t.base, t.n_blocks,
-                                                                     mlp, kappa_max);
+                                                                     mlp, kappa_max, measure, partials);
   }
 }
 
 cudaError_t launch_sweep_learned(const LaunchCtx &c, int geo, const BlockTable &half, const MlpDev *mlp,
-                                 float kappa_max) {
+                                 float kappa_max, int measure, double *partials) {
   if (half.n_blocks == 0) return cudaSuccess;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
@@ -592,11 +682,11 @@ cudaError_t launch_sweep_learned(const LaunchCtx &c, int geo, const BlockTable &
   const int grid = std::min(half.n_blocks, sms * 8);
   for (int colour = 0; colour < 2; colour++) {
     if (c.model.potential == POT_GHRL)
-      sweep_learned_pot<POT_GHRL>(c, geo, half, colour, mlp, kappa_max, grid);
+      sweep_learned_pot<POT_GHRL>(c, geo, half, colour, mlp, kappa_max, grid, measure, partials);
     else if (c.model.potential == POT_PEAR)
-      sweep_learned_pot<POT_PEAR>(c, geo, half, colour, mlp, kappa_max, grid);
+      sweep_learned_pot<POT_PEAR>(c, geo, half, colour, mlp, kappa_max, grid, measure, partials);
     else
-      sweep_learned_pot<POT_LL>(c, geo, half, colour, mlp, kappa_max, grid);
+      sweep_learned_pot<POT_LL>(c, geo, half, colour, mlp, kappa_max, grid, measure, partials);
   }
   return cudaGetLastError();
 }

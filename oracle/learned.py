@@ -8,7 +8,9 @@ What it restates (the algorithm the kernels implement, in plain numpy):
              yz, zz) and the temperature T; the site's own director is not an input, so the proposal is an
              independence proposal given the neighbours.
   network    7 -> 64 -> 64 -> 4 with SiLU, weights [out][in]; operands rounded to BF16 (features, weights, hidden
-             activations), products accumulated in FP32 by the kernels (here in FP64), biases FP32.
+             activations), products accumulated in FP32 by the kernels (here in FP64), biases FP32. The
+             activation is evaluated as h + h tanh(h), h = z / 2 in BF16 (silu_bf16); its gradient is the exact
+             SiLU derivative at z (straight through the rounding).
   head       axis mu = o[0:3] / |o[0:3]|, concentration kappa = clip(softplus(o[3]), KAPPA_MIN, kappa_max).
   proposal   q(n) = [ (1 - EPS) kappa cosh(kappa mu.n) / sinh(kappa) + EPS ] / (4 pi): an antipodally symmetrised
              von Mises-Fisher density mixed with EPS = 5 % uniform. Sampled by Wood's method (A. T. A. Wood,
@@ -103,16 +105,24 @@ def _rounders(rounding):
     return ident, ident
 
 
+def silu_bf16(z):
+    """The kernels' activation: z sigmoid(z) evaluated as h + h tanh(h) with h = z / 2 rounded to BF16, the result
+    rounded to BF16 (their tanh is the hardware approximation; here it is exact)."""
+    h = bf16(0.5 * np.asarray(z, np.float64))
+    return bf16(h + h * np.tanh(h))
+
+
 def forward(p, x, rounding=True):
     """Returns (out (n, 4), cache) with the BF16 rounding of the kernels (rounding=False: exact FP64, for
     finite-difference checks of the gradient formulas)."""
     r, rb = _rounders(rounding)
+    act = silu_bf16 if rounding else silu
     w1, b1, w2, b2, w3, b3 = unpack(p)
     xb = r(x)
     z1 = xb @ r(w1).T + rb(b1)
-    h1 = r(silu(z1))
+    h1 = act(z1)
     z2 = h1 @ r(w2).T + rb(b2)
-    h2 = r(silu(z2))
+    h2 = act(z2)
     o = h2 @ r(w3).T + rb(b3)
     return o, (xb, z1, h1, z2, h2)
 
