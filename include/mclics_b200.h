@@ -159,6 +159,30 @@ int mcl_debug_wait_limit(mcl_engine *e, long long timeout_ns, int withhold_first
  * director_field_*.csv. The mode may be given with or without the GPU suffix. */
 int mcl_run_input_file(const char *path);
 
+/* ---- Batched sweeps: tuning and graph replay (no counterpart in the reference: it runs one lattice per process,
+ * src/evolve.cu:317-440) ----------------------------------------------------------------------------------------
+ * The replicas of an engine are swept together: every work item (replica, tile, z segment) of every replica is one
+ * CTA of one launch. mcl_autotune times each candidate plan — tile configuration (64 x 14 sites with 256 threads
+ * per CTA, or 64 x 28 with 512) and planes per z segment — for trial_sweeps measured sweeps on the engine's own
+ * replicas, keeps the fastest and restores the directors, per-replica state, sweep counter and series, so the run
+ * continues as if it had not been called. MCL_ERR_STATE unless the engine runs the fused sweep (bulk/slab, plain
+ * proposal, no decision recording). */
+typedef struct mcl_tuning {
+  int tile_config;        /* 0 or 1 as above */
+  int rows_per_tile;
+  int threads_per_cta;
+  int planes_per_segment;
+  int work_items;         /* CTAs per sweep */
+  int candidates;         /* plans timed */
+  double ms_per_sweep;    /* the chosen plan: one sweep + its measurement */
+  double ms_default;      /* the plan in use before the call */
+} mcl_tuning;
+int mcl_autotune(mcl_engine *e, int trial_sweeps, mcl_tuning *out);
+/* With enable != 0, mcl_sweeps replays a captured CUDA graph of two fused sweeps (captured at the first call, again
+ * after the plan, the series buffer or the test hooks change) instead of launching kernels one by one; results are
+ * identical. Profiling (mcl_profile) uses direct launches. */
+int mcl_set_graphs(mcl_engine *e, int enable);
+
 /* ---- Learned Metropolis-Hastings proposal (no counterpart in the reference) ----------------------------------
  * Per site, a 7 -> 64 -> 64 -> 4 MLP with SiLU reads the neighbour Q-tensor sum sum_j (3 n_j n_j^T - I)/2 divided by
  * 6 (xx, xy, xz, yy, yz, zz) and T, and gives an axis mu (outputs 0..2, normalised) and a concentration

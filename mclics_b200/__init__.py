@@ -99,6 +99,8 @@ def lib():
             "mcl_debug_wait_limit": [vp, ctypes.c_longlong, i],
             "mcl_profile_read": [vp, P(ctypes.c_double), P(ctypes.c_longlong), P(ctypes.c_longlong)],
             "mcl_set_proposal": [vp, vp, f],
+            "mcl_autotune": [vp, i, P(CTuning)],
+            "mcl_set_graphs": [vp, i],
             "mcl_set_adaptation": [vp, i],
             "mcl_extract_samples": [vp, i, ctypes.c_longlong, ctypes.c_ulonglong, vp, vp],
             "mcl_mlp_forward": [vp, vp, ctypes.c_longlong, vp, vp],
@@ -179,6 +181,12 @@ def Replica(nx, ny, nz, geometry="bulk", periodic=(1, 1, 1), T=1.0, elecE=1.0, a
     r.periodic[:] = [int(bool(p)) for p in periodic]
     r.T, r.elecE, r.ang_var, r.seed = T, elecE, ang_var, seed
     return r
+
+
+class CTuning(ctypes.Structure):
+    _fields_ = [("tile_config", ctypes.c_int), ("rows_per_tile", ctypes.c_int), ("threads_per_cta", ctypes.c_int),
+                ("planes_per_segment", ctypes.c_int), ("work_items", ctypes.c_int), ("candidates", ctypes.c_int),
+                ("ms_per_sweep", ctypes.c_double), ("ms_default", ctypes.c_double)]
 
 
 class Engine:
@@ -310,6 +318,15 @@ class Engine:
             return
         p = mlp_params(params)
         check(lib().mcl_set_proposal(self._h, p.ctypes.data, kappa_max))
+
+    def autotune(self, trial_sweeps=3):
+        """Times the candidate tile plans on this engine's replicas, keeps the fastest (state is restored)."""
+        t = CTuning()
+        check(lib().mcl_autotune(self._h, trial_sweeps, ctypes.byref(t)))
+        return {k: getattr(t, k) for k, _ in CTuning._fields_}
+
+    def set_graphs(self, on=True):
+        check(lib().mcl_set_graphs(self._h, 1 if on else 0))
 
     def set_adaptation(self, on=True):
         check(lib().mcl_set_adaptation(self._h, 1 if on else 0))

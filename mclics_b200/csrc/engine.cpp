@@ -119,6 +119,47 @@ static int ensure_series(mcl_engine *e, int rows) {
   return MCL_OK;
 }
 
+// Captured sweep graphs hold kernel arguments (work items, buffers, series, test hooks): drop them whenever one of
+// those changes.
+static void drop_graphs(mcl_engine *e) {
+  for (int m = 0; m < 2; m++) {
+    if (e->graph[m]) cudaGraphExecDestroy(e->graph[m]);
+    e->graph[m] = nullptr;
+  }
+  e->graph_series = nullptr;
+}
+
+// Captures two fused sweeps (one per ping-pong parity, starting from buffer e->cur) as a graph. Every per-sweep
+// quantity the kernels use (sweep counter, temperatures, ang_var, series length) lives in device memory, so a
+// replay does exactly what two direct calls would.
+static int capture_graph(mcl_engine *e, int m) {
+  if (e->graph[m]) cudaGraphExecDestroy(e->graph[m]);
+  e->graph[m] = nullptr;
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+  const int cur0 = e->cur;
+  const long long l0 = e->launches;
+  int rc = fused_sweep(e, m != 0, nullptr, nullptr);
+  if (!rc) rc = fused_sweep(e, m != 0, nullptr, nullptr);
+  const cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
+  e->cur = cur0;
+  e->launches = l0;
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
+  const cudaError_t ie = cudaGraphInstantiate(&e->graph[m], g, 0);
+  cudaGraphDestroy(g);
+  if (ie != cudaSuccess) {
+    e->graph[m] = nullptr;
+    return cuda_fail(ie, "cudaGraphInstantiate");
+  }
+  e->graph_cur[m] = cur0;
+  if (m) e->graph_series = e->d_series;
+  return MCL_OK;
+}
+
 static int refresh_ghosts(mcl_engine *e) {
   if (!e->ghosts_dirty) return MCL_OK;
   CK(launch_refresh_ghosts(e->ctx(), 0, 0));
@@ -347,6 +388,7 @@ int mcl_create(const mcl_model *model, const mcl_replica *replicas, int n_replic
 int mcl_destroy(mcl_engine *e) {
   if (!e) return MCL_OK;
   if (e->stream) cudaStreamSynchronize(e->stream);
+  drop_graphs(e);
   if (e->fused) fused_destroy(e);
   free_table(e->half);
   free_table(e->boxes);
@@ -496,6 +538,22 @@ int mcl_sweeps(mcl_engine *e, int n, int measure) {
   if (measure && (rc = ensure_series(e, e->series_len + n))) return rc;
   const bool use_fused = e->fused && !e->record_dec && !e->d_mlp;
   if (use_fused && (rc = refresh_ghosts(e))) return rc;
+  if (use_fused && e->use_graphs && !e->profile && n >= 2) {
+    const int m = measure ? 1 : 0;
+    if (!e->graph[m] || (m && e->graph_series != (const void *)e->d_series)) {
+      if ((rc = capture_graph(e, m))) return rc;
+    }
+    if (e->cur != e->graph_cur[m]) {  // one direct sweep brings the buffers to the graph's parity
+      if ((rc = fused_sweep(e, measure != 0, nullptr, nullptr))) return rc;
+      if (measure) e->series_len++;
+      n--;
+    }
+    for (; n >= 2; n -= 2) {
+      CK(cudaGraphLaunch(e->graph[m], e->stream));
+      e->launches += 4;
+      if (measure) e->series_len += 2;
+    }
+  }
   for (int s = 0; s < n; s++) {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     if (e->profile) {
@@ -641,9 +699,111 @@ int mcl_synchronize(mcl_engine *e) {
 
 int mcl_debug_wait_limit(mcl_engine *e, long long timeout_ns, int withhold_first_load) {
   if (!e) return fail(MCL_ERR_ARG, "null engine");
+  drop_graphs(e);
   if (!e->fused) return fail(MCL_ERR_STATE, "this engine does not use the fused tiled sweep");
   fused_set_test_hooks(e, timeout_ns, withhold_first_load);
   return MCL_OK;
+}
+
+int mcl_set_graphs(mcl_engine *e, int enable) {
+  if (!e) return fail(MCL_ERR_ARG, "null engine");
+  CK(cudaStreamSynchronize(e->stream));
+  e->use_graphs = enable != 0;
+  if (!e->use_graphs) drop_graphs(e);
+  return MCL_OK;
+}
+
+int mcl_autotune(mcl_engine *e, int trial_sweeps, mcl_tuning *out) {
+  if (!e) return fail(MCL_ERR_ARG, "null engine");
+  if (trial_sweeps < 1 || trial_sweeps > 10000) return fail(MCL_ERR_ARG, "mcl_autotune: trial_sweeps outside 1..10000");
+  if (!e->fused || e->record_dec || e->d_mlp)
+    return fail(MCL_ERR_STATE, "mcl_autotune: the engine does not run the fused tiled sweep");
+  int rc;
+  if ((rc = ensure_series(e, e->series_len + trial_sweeps + 1))) return rc;
+  CK(cudaStreamSynchronize(e->stream));
+  // state to restore: directors (with ghosts), per-replica state, sweep counter, series length
+  float *save = nullptr;
+  CK(cudaMalloc(&save, (size_t)e->dir_floats * sizeof(float)));
+  const int cur0 = e->cur, series0 = e->series_len;
+  const bool graphs0 = e->use_graphs, prof0 = e->profile;
+  std::vector<RepState> st(e->n_rep);
+  unsigned long long sweep0 = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  auto done = [&](int code) {
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    cudaFree(save);
+    e->use_graphs = graphs0;
+    e->profile = prof0;
+    return code;
+  };
+#define CKT(call)                                                     \
+  do {                                                                \
+    cudaError_t e_ = (call);                                          \
+    if (e_ != cudaSuccess) return done(cuda_fail(e_, #call));         \
+  } while (0)
+  CKT(cudaMemcpyAsync(save, e->d_dir[cur0], (size_t)e->dir_floats * sizeof(float), cudaMemcpyDeviceToDevice,
+                      e->stream));
+  CKT(cudaMemcpyAsync(st.data(), e->d_state, e->n_rep * sizeof(RepState), cudaMemcpyDeviceToHost, e->stream));
+  CKT(cudaMemcpyAsync(&sweep0, e->d_sweep, sizeof sweep0, cudaMemcpyDeviceToHost, e->stream));
+  CKT(cudaStreamSynchronize(e->stream));
+  auto restore = [&]() -> int {
+    e->cur = cur0;
+    CK(cudaMemcpyAsync(e->d_dir[cur0], save, (size_t)e->dir_floats * sizeof(float), cudaMemcpyDeviceToDevice,
+                       e->stream));
+    CK(cudaMemcpyAsync(e->d_state, st.data(), e->n_rep * sizeof(RepState), cudaMemcpyHostToDevice, e->stream));
+    CK(cudaMemcpyAsync(e->d_sweep, &sweep0, sizeof sweep0, cudaMemcpyHostToDevice, e->stream));
+    CK(cudaMemcpyAsync(e->d_series_len, &series0, sizeof series0, cudaMemcpyHostToDevice, e->stream));
+    e->series_len = series0;
+    e->ghosts_dirty = false;  // the saved buffer carries its ghost cells
+    CK(cudaStreamSynchronize(e->stream));
+    return MCL_OK;
+  };
+  drop_graphs(e);
+  e->use_graphs = false;
+  e->profile = false;
+  CKT(cudaEventCreate(&ev0));
+  CKT(cudaEventCreate(&ev1));
+  int cfg0 = 0, seg0 = 0;
+  if ((rc = fused_get_cfg(e, &cfg0, nullptr, &seg0, nullptr))) return done(rc);
+  std::vector<std::pair<int, int>> cand;
+  fused_plan_candidates(e, cand);
+  if (std::find(cand.begin(), cand.end(), std::make_pair(cfg0, seg0)) == cand.end()) cand.push_back({cfg0, seg0});
+  double best = 1e300, t_default = 0;
+  std::pair<int, int> pick{cfg0, seg0};
+  for (const auto &c : cand) {
+    if ((rc = fused_set_plan(e, c.first, c.second))) return done(rc);
+    if ((rc = mcl_sweeps(e, 1, 1))) return done(rc);  // warm-up
+    CKT(cudaEventRecord(ev0, e->stream));
+    if ((rc = mcl_sweeps(e, trial_sweeps, 1))) return done(rc);
+    CKT(cudaEventRecord(ev1, e->stream));
+    CKT(cudaEventSynchronize(ev1));
+    float ms = 0.f;
+    CKT(cudaEventElapsedTime(&ms, ev0, ev1));
+    const double per = ms / trial_sweeps;
+    if (c.first == cfg0 && c.second == seg0) t_default = per;
+    if (per < best) {
+      best = per;
+      pick = c;
+    }
+    if ((rc = restore())) return done(rc);
+    if ((rc = fused_check_error(e))) return done(rc);
+  }
+  if ((rc = fused_set_plan(e, pick.first, pick.second))) return done(rc);
+  if (out) {
+    int ty = 0, seg = 0, items = 0;
+    fused_get_cfg(e, nullptr, &ty, &seg, &items);
+    out->tile_config = pick.first;
+    out->rows_per_tile = ty;
+    out->threads_per_cta = fused_threads(pick.first);
+    out->planes_per_segment = seg;
+    out->work_items = items;
+    out->candidates = (int)cand.size();
+    out->ms_per_sweep = best;
+    out->ms_default = t_default;
+  }
+#undef CKT
+  return done(MCL_OK);
 }
 
 int mcl_record_decisions(mcl_engine *e, int enable) {

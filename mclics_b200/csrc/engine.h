@@ -68,6 +68,10 @@ struct mcl_engine {
   mcl::MlpDev *d_mlp = nullptr;  // learned proposal (null: plain proposal)
   float kappa_max = 500.f;
   bool adapt = true;           // ang_var adaptation after each sweep (the reference's behaviour)
+  bool use_graphs = false;     // fused sweeps replayed from a captured CUDA graph of two sweeps
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};  // [measure]: two fused sweeps starting from buffer graph_cur
+  int graph_cur[2] = {0, 0};
+  const void *graph_series = nullptr;             // series buffer the measuring graph writes
 
   mcl::LaunchCtx ctx() const {
     mcl::LaunchCtx c;

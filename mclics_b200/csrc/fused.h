@@ -1,5 +1,8 @@
 // Fused two-colour tiled sweep (sweep_fused.cu): both colours of a sweep in one pass over HBM.
 #pragma once
+#include <utility>
+#include <vector>
+
 #include "engine.h"
 
 namespace mcl {
@@ -20,4 +23,9 @@ void fused_set_test_hooks(mcl_engine *e, long long timeout_ns, int skip_first_lo
 // Tile configuration of the fused sweep (0: 64 x 14 tiles, 256 threads, 2 CTAs/SM; 1: 64 x 30, 512 threads).
 int fused_set_cfg(mcl_engine *e, int cfg);
 int fused_get_cfg(const mcl_engine *e, int *cfg, int *ty, int *seg, int *items);
+// Tile configuration and planes per z segment (seg <= 0: the heuristic's choice); rebuilds the work items.
+int fused_set_plan(mcl_engine *e, int cfg, int seg);
+// Candidate (configuration, planes per segment) pairs for the autotuner, and the threads per CTA of a configuration.
+void fused_plan_candidates(const mcl_engine *e, std::vector<std::pair<int, int>> &out);
+int fused_threads(int cfg);
 }  // namespace mcl

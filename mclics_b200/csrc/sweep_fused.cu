@@ -15,6 +15,7 @@ static const FusedCfg kCfgs[kNumCfgs] = {{14, 256, 2}, {28, 512, 1}};
 
 struct FusedPlan {
   int cfg = 0, tx = 64, ty = 14, seg = 32;
+  int seg_override = 0;  // planes per z segment chosen by the autotuner (0: heuristic)
   int n_items = 0;
   FusedItem *d_items = nullptr;
   CUtensorMap *d_tmaps = nullptr;
@@ -94,6 +95,7 @@ static void choose_segments(const mcl_engine *e, FusedPlan &P, int sms) {
     }
   }
   P.seg = (int)((maxz + best - 1) / best);
+  if (P.seg_override > 0) P.seg = (int)std::min<long long>(P.seg_override, maxz);
 }
 
 static int choose_cfg(const mcl_engine *e) {
@@ -104,6 +106,8 @@ static int choose_cfg(const mcl_engine *e) {
   if (env) return std::max(0, std::min(kNumCfgs - 1, atoi(env)));
   return area >= 128ll * 128 ? 1 : 0;
 }
+
+static int prepare_kernel(mcl_engine *e, FusedPlan *P);
 
 static int build_items(mcl_engine *e, FusedPlan *P) {
   int sms = 148;
@@ -139,7 +143,7 @@ static int build_items(mcl_engine *e, FusedPlan *P) {
   CKF(cudaMalloc(&P->d_partials, (size_t)P->n_items * kPartials * sizeof(double)));
   const size_t slot_floats = ((size_t)3 * RW * (P->ty + 4) + 31) / 32 * 32;
   P->smem = 128 + (size_t)NSL * slot_floats * sizeof(float) + NSL * sizeof(unsigned long long);
-  return MCL_OK;
+  return prepare_kernel(e, P);
 }
 
 int fused_create(mcl_engine *e) {
@@ -160,6 +164,37 @@ int fused_set_cfg(mcl_engine *e, int cfg) {
   e->fused->cfg = cfg;
   return build_items(e, e->fused);
 }
+
+int fused_set_plan(mcl_engine *e, int cfg, int seg) {
+  if (!e->fused) return fail(MCL_ERR_STATE, "this engine does not use the fused tiled sweep");
+  if (cfg < 0 || cfg >= kNumCfgs) return fail(MCL_ERR_ARG, "tile configuration %d outside 0..%d", cfg, kNumCfgs - 1);
+  CKF(cudaStreamSynchronize(e->stream));
+  e->fused->cfg = cfg;
+  e->fused->seg_override = std::max(0, seg);
+  return build_items(e, e->fused);
+}
+
+void fused_plan_candidates(const mcl_engine *e, std::vector<std::pair<int, int>> &out) {
+  out.clear();
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device);
+  int maxz = 1;
+  for (auto &D : e->desc) maxz = std::max(maxz, D.nz);
+  for (int cfg = 0; cfg < kNumCfgs; cfg++) {
+    FusedPlan P;
+    P.cfg = cfg;
+    choose_segments(e, P, sms);
+    std::vector<int> segs = {P.seg, P.seg * 2, (P.seg + 1) / 2, maxz};
+    std::sort(segs.begin(), segs.end());
+    segs.erase(std::unique(segs.begin(), segs.end()), segs.end());
+    for (int sg : segs)
+      if (sg >= 6 || sg == maxz) out.push_back({cfg, std::min(sg, maxz)});
+  }
+  std::sort(out.begin(), out.end());
+  out.erase(std::unique(out.begin(), out.end()), out.end());
+}
+
+int fused_threads(int cfg) { return kCfgs[std::max(0, std::min(kNumCfgs - 1, cfg))].nt; }
 
 int fused_get_cfg(const mcl_engine *e, int *cfg, int *ty, int *seg, int *items) {
   if (!e->fused) return fail(MCL_ERR_STATE, "this engine does not use the fused tiled sweep");
@@ -182,6 +217,38 @@ void fused_destroy(mcl_engine *e) {
   e->fused = nullptr;
 }
 
+static FusedLaunch launch_desc(const mcl_engine *e, const FusedPlan *P) {
+  FusedLaunch l;
+  l.geo = e->geo;
+  l.cfg = P->cfg;
+  l.flip = e->model.flip != 0 || e->model.potential == POT_PEAR;
+  l.pxy = true;
+  for (const auto &D : e->desc) l.pxy = l.pxy && D.periodic[0] && D.periodic[1];
+  l.chiral = e->model.potential == POT_GHRL && e->model.sigma != 0.f;
+  l.field = e->model.field_on != 0;
+  l.n_items = P->n_items;
+  l.smem = P->smem;
+  l.stream = e->stream;
+  return l;
+}
+
+static cudaError_t dispatch(const mcl_engine *e, const FusedArgs &a, const FusedLaunch &l) {
+  if (e->model.potential == POT_GHRL) return launch_fused_ghrl(e->model, a, l);
+  if (e->model.potential == POT_PEAR) return launch_fused_pear(e->model, a, l);
+  return launch_fused_ll(e->model, a, l);
+}
+
+// Sets the dynamic shared-memory limit of the kernel this plan launches (once per plan, so that launches inside a
+// stream capture make no attribute calls).
+static int prepare_kernel(mcl_engine *e, FusedPlan *P) {
+  FusedLaunch l = launch_desc(e, P);
+  l.prepare = true;
+  FusedArgs a{};
+  const cudaError_t err = dispatch(e, a, l);
+  if (err != cudaSuccess) return cuda_fail(err, "fused sweep: shared-memory attribute");
+  return MCL_OK;
+}
+
 int fused_sweep(mcl_engine *e, bool measure, cudaEvent_t ev0, cudaEvent_t ev1) {
   FusedPlan *P = e->fused;
   FusedArgs a;
@@ -198,24 +265,8 @@ int fused_sweep(mcl_engine *e, bool measure, cudaEvent_t ev0, cudaEvent_t ev1) {
   a.timeout_ns = P->timeout_ns;
   a.skip_first_load = P->skip_first_load;
   if (ev0) CKF(cudaEventRecord(ev0, e->stream));
-  FusedLaunch l;
-  l.geo = e->geo;
-  l.cfg = P->cfg;
-  l.flip = e->model.flip != 0 || e->model.potential == POT_PEAR;
-  l.pxy = true;
-  for (const auto &D : e->desc) l.pxy = l.pxy && D.periodic[0] && D.periodic[1];
-  l.chiral = e->model.potential == POT_GHRL && e->model.sigma != 0.f;
-  l.field = e->model.field_on != 0;
-  l.n_items = P->n_items;
-  l.smem = P->smem;
-  l.stream = e->stream;
-  cudaError_t err;
-  if (e->model.potential == POT_GHRL)
-    err = launch_fused_ghrl(e->model, a, l);
-  else if (e->model.potential == POT_PEAR)
-    err = launch_fused_pear(e->model, a, l);
-  else
-    err = launch_fused_ll(e->model, a, l);
+  const FusedLaunch l = launch_desc(e, P);
+  const cudaError_t err = dispatch(e, a, l);
   if (err != cudaSuccess) return cuda_fail(err, "fused sweep launch");
   if (ev1) CKF(cudaEventRecord(ev1, e->stream));
   e->cur ^= 1;

@@ -530,6 +530,7 @@ struct FusedLaunch {
   int n_items;
   size_t smem;
   cudaStream_t stream;
+  bool prepare = false;  // only set the kernel's shared-memory limit (done once per plan, outside any capture)
 };
 cudaError_t launch_fused_ll(const ModelDev &m, const FusedArgs &a, const FusedLaunch &l);
 cudaError_t launch_fused_ghrl(const ModelDev &m, const FusedArgs &a, const FusedLaunch &l);
@@ -538,8 +539,7 @@ cudaError_t launch_fused_pear(const ModelDev &m, const FusedArgs &a, const Fused
 template <int POT, int GEO, bool FLIP, bool PXY, bool CHIRAL, bool FIELD, int TY, int NT>
 cudaError_t launch_fused_one(const ModelDev &m, const FusedArgs &a, const FusedLaunch &l) {
   auto k = k_sweep_fused<POT, GEO, FLIP, PXY, CHIRAL, FIELD, TY, NT>;
-  cudaError_t err = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)l.smem);
-  if (err != cudaSuccess) return err;
+  if (l.prepare) return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)l.smem);
   k<<<l.n_items, NT, l.smem, l.stream>>>(m, a);
   return cudaGetLastError();
 }

@@ -38,7 +38,8 @@ def test_struct_layouts_match_header(tmp_path):
     import subprocess
     src = tmp_path / "sz.c"
     checks = []
-    for cname, py in (("mcl_model", M.CModel), ("mcl_replica", M.CReplica), ("mcl_observables", M.CObservables)):
+    for cname, py in (("mcl_model", M.CModel), ("mcl_replica", M.CReplica), ("mcl_observables", M.CObservables),
+                      ("mcl_tuning", M.CTuning)):
         checks.append('printf("%%s %%zu\\n", "%s", sizeof(%s));' % (cname, cname))
         for f, _ in py._fields_:
             checks.append('printf("%%s.%%s %%zu\\n", "%s", "%s", offsetof(%s, %s));' % (cname, f, cname, f))
@@ -48,7 +49,8 @@ def test_struct_layouts_match_header(tmp_path):
     subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
     out = dict(l.rsplit(" ", 1) for l in subprocess.run([str(exe)], capture_output=True, text=True,
                                                          check=True).stdout.split("\n") if l)
-    for cname, py in (("mcl_model", M.CModel), ("mcl_replica", M.CReplica), ("mcl_observables", M.CObservables)):
+    for cname, py in (("mcl_model", M.CModel), ("mcl_replica", M.CReplica), ("mcl_observables", M.CObservables),
+                      ("mcl_tuning", M.CTuning)):
         assert int(out[cname]) == ctypes.sizeof(py), cname
         for f, _ in py._fields_:
             assert int(out["%s.%s" % (cname, f)]) == getattr(py, f).offset, (cname, f)
@@ -103,3 +105,14 @@ def test_input_errors_leave_old_output(name, params, text, tmp_path, capfd):
     assert text in err, err
     assert ei.value.code in (1, 5)
     assert open(os.path.join(d, "po.dat")).read() == "old results\n"
+
+
+def test_mlp_struct_is_the_flat_parameter_vector(tmp_path):
+    import subprocess
+    src = tmp_path / "m.c"
+    src.write_text('#include <stdio.h>\n#include "mclics_b200.h"\nint main(void){printf("%zu\\n", sizeof(mcl_mlp));'
+                   'return 0;}\n')
+    exe = tmp_path / "m"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout
+    assert int(out) == 4 * M.N_MLP_PARAMS
