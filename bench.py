@@ -9,7 +9,9 @@ measurement (energy, Q tensor, S, acceptance, device-side ang_var adaptation), i
 reference's thermalGPU loop. Metric: site updates per second (whole job, all GPUs).
 
   value      device time (CUDA events on the engine's stream) of K steps with the lattice resident in HBM. The
-             lattice (211 MB padded) is larger than L2 (126 MB), so no flush is needed between steps.
+             lattice (211 MB padded) is larger than L2 (126 MB), so no flush is needed between steps. The tile
+             plan is chosen by mcl_autotune before timing, and the K steps are one mcl_sweeps call replaying a
+             captured CUDA graph of the fused sweeps.
   e2e        the same steps through the C ABI as the reference's GPU mode loop drives them, host buffers and
              host<->device copies inside the timed region: per step the temperature goes up from pinned host
              memory, the observables record and the whole director field (the reference copies it back after
@@ -260,27 +262,36 @@ def gpu_arm(args, rank, world, local_rank):
     for _ in range(args.warmup):
         eng.sweeps(1, measure=True)
     eng.synchronize()
+    # tile plan by the autotuner (state restored), then graph replay of the fused sweeps
+    tuning = eng.autotune(3)
+    eng.set_graphs(True)
+    eng.sweeps(2, measure=True)  # captures the graph outside the timed region
+    eng.synchronize()
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
 
     clocks = ClockSampler(local_rank)
     clocks.start()
-    eng.profile(True)
-    ms0, n0, l0 = eng.profile_read()
+    _, _, l0 = eng.profile_read()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(args.steps):
-        eng.sweeps(1, measure=True)
+    eng.sweeps(args.steps, measure=True)  # K steps = K sweeps, each with its measurement
     e1.record(stream)
     e1.synchronize()
     clocks.stop()
     dev_ms = e0.elapsed_time(e1)
-    ms1, n1, l1 = eng.profile_read()
+    _, _, l1 = eng.profile_read()
+    launches = l1 - l0
+    # sweep-kernel time for the roofline: a separate run with per-sweep events (direct launches)
+    eng.profile(True)
+    ms0, n0, _ = eng.profile_read()
+    eng.sweeps(min(args.steps, 50), measure=True)
+    eng.synchronize()
+    ms1, n1, _ = eng.profile_read()
     eng.profile(False)
     kernel_ms = (ms1 - ms0) / max(1, n1 - n0)
-    launches = l1 - l0
     rec = eng.series(0, eng.series_length() - 1, 1)[0]
 
     # end to end through the C ABI with host buffers (reference GPU loop data movement, all replicas)
@@ -308,7 +319,7 @@ def gpu_arm(args, rank, world, local_rank):
     eng.close()
     return dict(dev_ms=dev_ms_max, e2e_ms=e2e_ms_max, kernel_ms=kernel_ms, launches=launches, sites=sites,
                 n_rep=len(reps), clocks=clocks.summary(), S=float(rec["S"]), E=float(rec["energy"]),
-                acc=float(rec["acceptance"]), cfg=cfg)
+                acc=float(rec["acceptance"]), cfg=cfg, tuning=tuning)
 
 
 def learned_compare(args):
@@ -469,6 +480,10 @@ def main():
         return 0
     sites_total = res["sites"] * world
     config["global_sites_per_step"] = sites_total
+    tu = res["tuning"]
+    config["plan"] = {"autotuned": True, "rows_per_tile": tu["rows_per_tile"], "threads_per_cta": tu["threads_per_cta"],
+                      "planes_per_segment": tu["planes_per_segment"], "ctas": tu["work_items"],
+                      "candidates": tu["candidates"], "cuda_graph": True}
     config["l2"] = ("inputs larger than L2 (%.0f MB of directors > 126 MB)" % (res["sites"] * 12 / 1e6)
                     if res["sites"] * 12 > 126e6 else
                     "inputs smaller than L2 (%.0f MB): DRAM roofline is an upper bound" % (res["sites"] * 12 / 1e6))
