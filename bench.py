@@ -250,7 +250,15 @@ def gpu_arm(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     model, reps, cfg, ic = workload(args.workload)
-    creps = [M.Replica(**dict(r, seed=r["seed"] + 1000 * rank)) for r in reps]
+    all_sites = sum(r["nx"] * r["ny"] * r["nz"] for r in reps)
+    if args.shard and world > 1:  # strong scaling: this rank's share of the batch, largest replicas first
+        from mclics_b200 import sharding
+        if len(reps) < world:
+            raise SystemExit("--shard needs at least one replica per rank (%d replicas, %d ranks)" % (len(reps), world))
+        reps = [reps[i] for i in sharding.shard([r["nx"] * r["ny"] * r["nz"] for r in reps], world, rank)]
+        creps = [M.Replica(**r) for r in reps]
+    else:  # weak scaling: every rank sweeps its own copy of the workload
+        creps = [M.Replica(**dict(r, seed=r["seed"] + 1000 * rank)) for r in reps]
     eng = M.Engine(model, creps)
     sizes = [r["nx"] * r["ny"] * r["nz"] for r in reps]
     for i, n in enumerate(sizes):
@@ -318,6 +326,7 @@ def gpu_arm(args, rank, world, local_rank):
     dev_ms_max, e2e_ms_max = float(times[0]), float(times[1])
     eng.close()
     return dict(dev_ms=dev_ms_max, e2e_ms=e2e_ms_max, kernel_ms=kernel_ms, launches=launches, sites=sites,
+                all_sites=all_sites,
                 n_rep=len(reps), clocks=clocks.summary(), S=float(rec["S"]), E=float(rec["energy"]),
                 acc=float(rec["acceptance"]), cfg=cfg, tuning=tuning)
 
@@ -421,6 +430,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="mclics_b200", choices=["mclics_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--shard", action="store_true",
+                    help="N > 1: split the workload's replicas across ranks (strong scaling) instead of one copy per rank")
     ap.add_argument("--learned", action="store_true",
                     help="learned vs plain proposal: train the proposal network, compare ESS/s of E and S")
     ap.add_argument("--ess-sweeps", type=int, default=10000)
@@ -439,7 +450,8 @@ def main():
         return learned_compare(args)
     _, _, config, _ = workload(args.workload) if args.impl != "reference" else workload("c2")
     config = dict(config, step="1 sweep + measurement of every lattice", accumulators="f64 (energy, Q, sum n)",
-                  parallelism="independent replicas x%d" % max(1, args.gpus))
+                  parallelism=("replicas split across %d GPUs" % args.gpus if args.shard and args.gpus > 1
+                               else "independent replicas x%d" % max(1, args.gpus)))
 
     if args.impl == "reference":
         if rank != 0:
@@ -481,7 +493,8 @@ def main():
         torch.distributed.destroy_process_group()
     if rank != 0:
         return 0
-    sites_total = res["sites"] * world
+    sharded = args.shard and world > 1
+    sites_total = res["all_sites"] if sharded else res["sites"] * world
     config["global_sites_per_step"] = sites_total
     tu = res["tuning"]
     config["plan"] = {"autotuned": True, "rows_per_tile": tu["rows_per_tile"], "threads_per_cta": tu["threads_per_cta"],
@@ -496,7 +509,8 @@ def main():
     achieved = res["sites"] * BYTES_PER_SITE_UPDATE / (res["kernel_ms"] / 1e3) / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": "site-updates/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": res["dev_ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": res["dev_ms"] / args.steps, "higher_is_better": True,
+        "scaling": "strong" if sharded else "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config,
         "e2e": {"value": e2e, "unit": "site-updates/s", "h2d_bytes_per_step": 4 * res["n_rep"],
                 "d2h_bytes_per_step": 144 * res["n_rep"] + 12 * res["sites"]},

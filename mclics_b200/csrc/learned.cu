@@ -96,14 +96,17 @@ __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
 __device__ __forceinline__ uint32_t ld32(const __nv_bfloat16 *p) { return *reinterpret_cast<const uint32_t *>(p); }
 
 // SiLU of two halved pre-activations h = z / 2 (FP32), returned as packed BF16 (low half: the first):
-// z sigmoid(z) = h + h tanh(h) with h rounded to BF16, i.e. one tanh.approx.bf16x2 and one bf16x2 fma per pair.
-// Inference and training both use exactly this.
+// z sigmoid(z) = h + h tanh(h), with the hardware tanh approximation in FP32 and one paired FP32 fma, rounded once
+// to BF16. Inference and training both use exactly this.
+__device__ __forceinline__ float tanh_hw(float h) {
+  float t;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(h));
+  return t;
+}
 __device__ __forceinline__ uint32_t silu2h(float h0, float h1) {
-  const uint32_t h = pack2(h0, h1);
-  uint32_t t, r;
-  asm("tanh.approx.bf16x2 %0, %1;" : "=r"(t) : "r"(h));
-  asm("fma.rn.bf16x2 %0, %1, %2, %1;" : "=r"(r) : "r"(h), "r"(t));
-  return r;
+  const float2 h = make_float2(h0, h1);
+  const float2 r = __ffma2_rn(h, make_float2(tanh_hw(h0), tanh_hw(h1)), h);
+  return pack2(r.x, r.y);
 }
 __device__ __forceinline__ uint32_t silu2(float z0, float z1) { return silu2h(0.5f * z0, 0.5f * z1); }
 
@@ -328,13 +331,13 @@ __global__ void __launch_bounds__(kThreads, 3) k_sweep_learned(ModelDev m, const
       nb[d] = Vec3{0.f, 0.f, 0.f};
       w[d] = 0.f;
     }
-    if (q < total) {
-      const int xh = (int)(q % hx);
-      const long long row = q / hx;
-      y = (int)(row % R.ny);
-      z = (int)(row / R.ny);
+    if (q < total) {  // a replica has fewer than 2^32 sites (checked at creation): 32-bit decode
+      const unsigned qq = (unsigned)q, row = qq / (unsigned)hx;
+      const int xh = (int)(qq - row * (unsigned)hx);
+      z = (int)(row / (unsigned)R.ny);
+      y = (int)(row - (unsigned)z * (unsigned)R.ny);
       x = 2 * xh + ((colour + y + z) & 1);
-      if (x < R.nx) valid = gather_site_w<GEO>(R, dir, pt, nrm, x, y, z, n, nb, w, sid, s);
+      if (x < R.nx) valid = gather_site_rows<GEO>(R, dir, pt, nrm, x, y, z, n, nb, w, sid, s);
     }
     float f[kIn] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     if (valid) site_features(nb, w, St.T, f);
@@ -448,7 +451,7 @@ __global__ void k_extract_samples(const RepDesc *__restrict__ reps, const RepSta
   float w[6];
   int sid;
   float f[kIn] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  const bool valid = gather_site_w<GEO>(R, dir, pt, nrm, x, y, z, nv, nb, w, sid, s);
+  const bool valid = gather_site_rows<GEO>(R, dir, pt, nrm, x, y, z, nv, nb, w, sid, s);
   if (valid) site_features(nb, w, st[rep].T, f);
 #pragma unroll
   for (int k = 0; k < kIn; k++) feat[i * kFeat + k] = f[k];

@@ -9,8 +9,8 @@ What it restates (the algorithm the kernels implement, in plain numpy):
              independence proposal given the neighbours.
   network    7 -> 64 -> 64 -> 4 with SiLU, weights [out][in]; operands rounded to BF16 (features, weights, hidden
              activations), products accumulated in FP32 by the kernels (here in FP64), biases FP32. The
-             activation is evaluated as h + h tanh(h), h = z / 2 in BF16 (silu_bf16); its gradient is the exact
-             SiLU derivative at z (straight through the rounding).
+             activation is evaluated as h + h tanh(h), h = z / 2, then rounded to BF16 (silu_bf16); its gradient
+             is the exact SiLU derivative at z (straight through the rounding).
   head       axis mu = o[0:3] / |o[0:3]|, concentration kappa = clip(softplus(o[3]), KAPPA_MIN, kappa_max).
   proposal   q(n) = [ (1 - EPS) kappa cosh(kappa mu.n) / sinh(kappa) + EPS ] / (4 pi): an antipodally symmetrised
              von Mises-Fisher density mixed with EPS = 5 % uniform. Sampled by Wood's method (A. T. A. Wood,
@@ -106,9 +106,9 @@ def _rounders(rounding):
 
 
 def silu_bf16(z):
-    """The kernels' activation: z sigmoid(z) evaluated as h + h tanh(h) with h = z / 2 rounded to BF16, the result
-    rounded to BF16 (their tanh is the hardware approximation; here it is exact)."""
-    h = bf16(0.5 * np.asarray(z, np.float64))
+    """The kernels' activation: z sigmoid(z) evaluated as h + h tanh(h) with h = z / 2, the result rounded to BF16
+    (their tanh is the hardware approximation; here it is exact)."""
+    h = 0.5 * np.asarray(z, np.float64)
     return bf16(h + h * np.tanh(h))
 
 
