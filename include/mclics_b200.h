@@ -159,6 +159,19 @@ int mcl_debug_wait_limit(mcl_engine *e, long long timeout_ns, int withhold_first
  * director_field_*.csv. The mode may be given with or without the GPU suffix. */
 int mcl_run_input_file(const char *path);
 
+/* Extra order parameters of the current state of one replica, on the device (Polarization, Splay_magnitude,
+ * Splay_divergence, Radial_order of src/parameter_order.cpp:129-245; the reference computes them on the host after
+ * copying the lattice back, src/parameter_order.cpp:249-295). director: the Q-tensor director of the same state
+ * (mcl_observables.director), for P = |d . sum n| / N_valid. Radial orders are about the grid centre
+ * (Nx/2, Ny/2, Nz/2) and about the z axis through it, skipping sites within half a spacing. The first call allocates
+ * scratch for the engine's largest replica. Synchronises. */
+typedef struct mcl_extras {
+  double P, dtheta, divn;
+  double Sr_sph, Pr_sph;  /* about the centre */
+  double Sr_cyl, Pr_cyl;  /* about the z axis */
+} mcl_extras;
+int mcl_measure_extras(mcl_engine *e, int replica, const double director[3], mcl_extras *out);
+
 /* ---- Batched sweeps: tuning and graph replay (no counterpart in the reference: it runs one lattice per process,
  * src/evolve.cu:317-440) ----------------------------------------------------------------------------------------
  * The replicas of an engine are swept together: every work item (replica, tile, z segment) of every replica is one

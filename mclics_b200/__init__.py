@@ -100,6 +100,7 @@ def lib():
             "mcl_profile_read": [vp, P(ctypes.c_double), P(ctypes.c_longlong), P(ctypes.c_longlong)],
             "mcl_set_proposal": [vp, vp, f],
             "mcl_autotune": [vp, i, P(CTuning)],
+            "mcl_measure_extras": [vp, i, P(ctypes.c_double * 3), P(CExtras)],
             "mcl_set_graphs": [vp, i],
             "mcl_set_adaptation": [vp, i],
             "mcl_extract_samples": [vp, i, ctypes.c_longlong, ctypes.c_ulonglong, vp, vp],
@@ -181,6 +182,10 @@ def Replica(nx, ny, nz, geometry="bulk", periodic=(1, 1, 1), T=1.0, elecE=1.0, a
     r.periodic[:] = [int(bool(p)) for p in periodic]
     r.T, r.elecE, r.ang_var, r.seed = T, elecE, ang_var, seed
     return r
+
+
+class CExtras(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in ("P", "dtheta", "divn", "Sr_sph", "Pr_sph", "Sr_cyl", "Pr_cyl")]
 
 
 class CTuning(ctypes.Structure):
@@ -318,6 +323,13 @@ class Engine:
             return
         p = mlp_params(params)
         check(lib().mcl_set_proposal(self._h, p.ctypes.data, kappa_max))
+
+    def measure_extras(self, r, director):
+        """P, dtheta, divn and the radial orders of replica r's current state (director: that state's Q director)."""
+        d = (ctypes.c_double * 3)(*[float(v) for v in director])
+        x = CExtras()
+        check(lib().mcl_measure_extras(self._h, r, ctypes.byref(d), ctypes.byref(x)))
+        return {k: getattr(x, k) for k, _ in CExtras._fields_}
 
     def autotune(self, trial_sweeps=3):
         """Times the candidate tile plans on this engine's replicas, keeps the fastest (state is restored)."""

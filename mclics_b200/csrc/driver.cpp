@@ -750,13 +750,29 @@ int print_n(const char *fname, const Params &p, const Setup &s, const float *ni)
   return MCL_OK;
 }
 
-// Extra po.dat columns (src/parameter_order.cpp:129-295). P uses the device's FP64 sum of n and the director of
-// the same sweep; dtheta, divn and the radial orders need the lattice and are computed on the host.
+// Extra po.dat columns (src/parameter_order.cpp:129-295), computed on the device after every measurement sweep
+// (mcl_measure_extras) and accumulated as ExtraObservables::accumulate does (P, dtheta, divn rounded to float, the
+// radial orders in double).
 struct Extras {
   bool pear, sph, cyl;
   double P = 0, dTheta = 0, divN = 0, SrS = 0, PrS = 0, SrC = 0, PrC = 0;
   void reset() { P = dTheta = divN = SrS = PrS = SrC = PrC = 0; }
-  bool needs_lattice() const { return pear || sph || cyl; }
+  bool any() const { return pear || sph || cyl; }
+  void add(const mcl_extras &x) {
+    if (pear) {
+      P += (float)x.P;
+      dTheta += (float)x.dtheta;
+      divN += (float)x.divn;
+    }
+    if (sph) {
+      SrS += x.Sr_sph;
+      PrS += x.Pr_sph;
+    }
+    if (cyl) {
+      SrC += x.Sr_cyl;
+      PrC += x.Pr_cyl;
+    }
+  }
   void header(FILE *f) const {
     if (pear) fprintf(f, " P dtheta divn");
     if (sph) fprintf(f, pear ? " Sr_sph Pr_sph" : " Sr_sph");
@@ -776,99 +792,6 @@ struct Extras {
     fprintf(f, "\n");
   }
 };
-
-void radial(const Params &p, const Setup &s, const float *ni, bool cylinder, double &Sr, double &Pr) {
-  const float cx = p.Nx / 2, cy = p.Ny / 2, cz = p.Nz / 2;
-  double sS = 0, sP = 0;
-  long valid = 0;
-  for (int k = 0; k < p.Nz; k++)
-    for (int j = 0; j < p.Ny; j++)
-      for (int i = 0; i < p.Nx; i++) {
-        long long q = i + (long long)p.Nx * (j + (long long)p.Ny * k);
-        if (!s.pt[q]) continue;
-        const float rx = i - cx, ry = j - cy, rz = cylinder ? 0 : k - cz;
-        const float r = sqrtf(rx * rx + ry * ry + rz * rz);
-        if (r < 0.5f) continue;
-        const double c = (ni[3 * q] * rx + ni[3 * q + 1] * ry + ni[3 * q + 2] * rz) / r;
-        sS += 1.5 * c * c - 0.5;
-        sP += c;
-        valid++;
-      }
-  Sr = valid ? sS / valid : 0;
-  Pr = valid ? sP / valid : 0;
-}
-
-void accumulate_extras(Extras &x, const Params &p, const Setup &s, const float *ni, const mcl_observables &o) {
-  if (x.pear) {
-    // Polarization: |d . sum n| / N_valid with d = director (float) of this sweep
-    const float d[3] = {(float)o.director[0], (float)o.director[1], (float)o.director[2]};
-    double sum = 0;
-    long long valid = 0;
-    const long long Nt = (long long)p.Nx * p.Ny * p.Nz;
-    for (long long q = 0; q < Nt; q++) {
-      if (!s.pt[q]) continue;
-      sum += d[0] * ni[3 * q] + d[1] * ni[3 * q + 1] + d[2] * ni[3 * q + 2];
-      valid++;
-    }
-    x.P += (float)(valid ? fabs(sum) / valid : 0);
-    // splay vector magnitude (parameter_order.cpp:147-176)
-    static const int dirs[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
-    double sv[3] = {0, 0, 0};
-    long nB = 0;
-    double sumdiv = 0;
-    long validd = 0;
-    for (int k = 0; k < p.Nz; k++)
-      for (int j = 0; j < p.Ny; j++)
-        for (int i = 0; i < p.Nx; i++) {
-          const long long idx = i + (long long)p.Nx * (j + (long long)p.Ny * k);
-          if (!s.pt[idx]) continue;
-          const float *a = &ni[3 * idx];
-          for (int d6 = 0; d6 < 6; d6++) {
-            int ii = i + dirs[d6][0], jj = j + dirs[d6][1], kk = k + dirs[d6][2];
-            if (!(bnd(s.periodic[0], ii, p.Nx) && bnd(s.periodic[1], jj, p.Ny) && bnd(s.periodic[2], kk, p.Nz))) continue;
-            const long long jdx = ii + (long long)p.Nx * (jj + (long long)p.Ny * kk);
-            if (!s.pt[jdx]) continue;
-            const float *b = &ni[3 * jdx];
-            const float ra = a[0] * dirs[d6][0] + a[1] * dirs[d6][1] + a[2] * dirs[d6][2];
-            const float rb = b[0] * dirs[d6][0] + b[1] * dirs[d6][1] + b[2] * dirs[d6][2];
-            const float ab = a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
-            for (int c = 0; c < 3; c++) sv[c] += 0.5 * (b[c] * rb - a[c] * ra + a[c] * ab * rb - b[c] * ab * ra);
-            nB++;
-          }
-          // divergence (parameter_order.cpp:183-215)
-          double div = 0;
-          for (int ax = 0; ax < 3; ax++) {
-            double dd = 0;
-            int nb = 0;
-            for (int sg = -1; sg <= 1; sg += 2) {
-              int ii = i, jj = j, kk = k;
-              if (ax == 0) ii += sg; else if (ax == 1) jj += sg; else kk += sg;
-              if (!(bnd(s.periodic[0], ii, p.Nx) && bnd(s.periodic[1], jj, p.Ny) && bnd(s.periodic[2], kk, p.Nz))) continue;
-              const long long jdx = ii + (long long)p.Nx * (jj + (long long)p.Ny * kk);
-              if (!s.pt[jdx]) continue;
-              dd += sg * (ni[3 * jdx + ax] - ni[3 * idx + ax]);
-              nb++;
-            }
-            if (nb) div += dd / nb;
-          }
-          sumdiv += div;
-          validd++;
-        }
-    x.dTheta += (float)(nB ? 1.5 * sqrt(sv[0] * sv[0] + sv[1] * sv[1] + sv[2] * sv[2]) / nB : 0);
-    x.divN += (float)(validd ? sumdiv / validd : 0);
-  }
-  double sr, pr;
-  if (x.sph) {
-    radial(p, s, ni, false, sr, pr);
-    x.SrS += sr;
-    x.PrS += pr;
-  }
-  if (x.cyl) {
-    radial(p, s, ni, true, sr, pr);
-    x.SrC += sr;
-    x.PrC += pr;
-  }
-}
 
 void clean_previous_output() {
   printf("  Removing output files from previous run... ");
@@ -905,18 +828,17 @@ int measure_block(mcl_engine *e, const Params &p, const Setup &s, Extras &ex, st
                   BlockResult &r) {
   RUN_CK(mcl_clear_series(e));
   std::vector<mcl_observables> obs;
-  if (ex.needs_lattice()) {
-    // the extra observables need the whole lattice after every sweep, as in the reference
-    obs.resize(1);
+  if (ex.any()) {
+    // the extra observables of the state after every measurement sweep, as in the reference
     for (int step = 0; step < p.MCS; step++) {
       RUN_CK(mcl_sweeps(e, 1, 1));
       mcl_observables o;
       RUN_CK(mcl_read_series(e, 0, step, 1, &o));
-      RUN_CK(mcl_download_directors(e, 0, host_ni.data()));
-      accumulate_extras(ex, p, s, host_ni.data(), o);
+      mcl_extras x;
+      RUN_CK(mcl_measure_extras(e, 0, o.director, &x));
+      ex.add(x);
       obs.push_back(o);
     }
-    obs.erase(obs.begin());
   } else {
     RUN_CK(mcl_sweeps(e, p.MCS, 1));
     obs.resize(p.MCS);

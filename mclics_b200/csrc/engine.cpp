@@ -396,6 +396,7 @@ int mcl_destroy(mcl_engine *e) {
   cudaFree(e->d_dir[0]);
   cudaFree(e->d_dir[1]);
   cudaFree(e->d_mlp);
+  cudaFree(e->d_xpart);
   cudaFree(e->d_pt);
   cudaFree(e->d_nrm);
   cudaFree(e->d_stage);

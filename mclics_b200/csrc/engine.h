@@ -66,6 +66,7 @@ struct mcl_engine {
   long long prof_sweeps = 0;
   long long launches = 0;      // kernels launched by this engine
   mcl::MlpDev *d_mlp = nullptr;  // learned proposal (null: plain proposal)
+  double *d_xpart = nullptr;   // scratch of mcl_measure_extras (allocated at its first call)
   float kappa_max = 500.f;
   bool adapt = true;           // ang_var adaptation after each sweep (the reference's behaviour)
   bool use_graphs = false;     // fused sweeps replayed from a captured CUDA graph of two sweeps

@@ -39,7 +39,7 @@ def test_struct_layouts_match_header(tmp_path):
     src = tmp_path / "sz.c"
     checks = []
     for cname, py in (("mcl_model", M.CModel), ("mcl_replica", M.CReplica), ("mcl_observables", M.CObservables),
-                      ("mcl_tuning", M.CTuning)):
+                      ("mcl_tuning", M.CTuning), ("mcl_extras", M.CExtras)):
         checks.append('printf("%%s %%zu\\n", "%s", sizeof(%s));' % (cname, cname))
         for f, _ in py._fields_:
             checks.append('printf("%%s.%%s %%zu\\n", "%s", "%s", offsetof(%s, %s));' % (cname, f, cname, f))
@@ -50,7 +50,7 @@ def test_struct_layouts_match_header(tmp_path):
     out = dict(l.rsplit(" ", 1) for l in subprocess.run([str(exe)], capture_output=True, text=True,
                                                          check=True).stdout.split("\n") if l)
     for cname, py in (("mcl_model", M.CModel), ("mcl_replica", M.CReplica), ("mcl_observables", M.CObservables),
-                      ("mcl_tuning", M.CTuning)):
+                      ("mcl_tuning", M.CTuning), ("mcl_extras", M.CExtras)):
         assert int(out[cname]) == ctypes.sizeof(py), cname
         for f, _ in py._fields_:
             assert int(out["%s.%s" % (cname, f)]) == getattr(py, f).offset, (cname, f)
