@@ -171,6 +171,11 @@ typedef struct mcl_extras {
   double Sr_cyl, Pr_cyl;  /* about the z axis */
 } mcl_extras;
 int mcl_measure_extras(mcl_engine *e, int replica, const double director[3], mcl_extras *out);
+/* Local order parameter of every site of one replica, on the device (lattice_order_parameter,
+ * src/parameter_order.cpp:75-127, written in every snapshot by print_n, src/io.cpp:59-89): the largest eigenvalue
+ * of Q over the site and its existing non-empty neighbours; NaN on empty sites. S: host array of Nx Ny Nz floats in
+ * the reference order. Synchronises. */
+int mcl_local_order(mcl_engine *e, int replica, float *S);
 
 /* ---- Batched sweeps: tuning and graph replay (no counterpart in the reference: it runs one lattice per process,
  * src/evolve.cu:317-440) ----------------------------------------------------------------------------------------

@@ -101,6 +101,7 @@ def lib():
             "mcl_set_proposal": [vp, vp, f],
             "mcl_autotune": [vp, i, P(CTuning)],
             "mcl_measure_extras": [vp, i, P(ctypes.c_double * 3), P(CExtras)],
+            "mcl_local_order": [vp, i, vp],
             "mcl_set_graphs": [vp, i],
             "mcl_set_adaptation": [vp, i],
             "mcl_extract_samples": [vp, i, ctypes.c_longlong, ctypes.c_ulonglong, vp, vp],
@@ -330,6 +331,12 @@ class Engine:
         x = CExtras()
         check(lib().mcl_measure_extras(self._h, r, ctypes.byref(d), ctypes.byref(x)))
         return {k: getattr(x, k) for k, _ in CExtras._fields_}
+
+    def local_order(self, r):
+        """Local order parameter S of every site of replica r (NaN on empty sites), reference order."""
+        out = np.empty(self.sites(r), np.float32)
+        check(lib().mcl_local_order(self._h, r, out.ctypes.data))
+        return out
 
     def autotune(self, trial_sweeps=3):
         """Times the candidate tile plans on this engine's replicas, keeps the fastest (state is restored)."""

@@ -729,8 +729,9 @@ float local_S(const Params &p, const Setup &s, const float *ni, int i, int j, in
   return (float)mcl::largest_eigen3(qd, v);
 }
 
-// Snapshot / ic.csv (src/io.cpp:59-89).
-int print_n(const char *fname, const Params &p, const Setup &s, const float *ni) {
+// Snapshot / ic.csv (src/io.cpp:59-89). S: the local order parameters from the device (mcl_local_order), or null
+// to compute them here (ic.csv, written before the engine exists).
+int print_n(const char *fname, const Params &p, const Setup &s, const float *ni, const float *S = nullptr) {
   FILE *f = fopen(fname, "w");
   if (!f) {
     perror(fname);
@@ -741,8 +742,8 @@ int print_n(const char *fname, const Params &p, const Setup &s, const float *ni)
     for (int j = 0; j < p.Ny; j++)
       for (int i = 0; i < p.Nx; i++) {
         long long q = i + (long long)p.Nx * (j + (long long)p.Ny * k);
-        float S = s.pt[q] ? local_S(p, s, ni, i, j, k) : NAN;
-        fprintf(f, "%d,%d,%d,%g,%g,%g,%g,%d\n", i, j, k, ni[3 * q], ni[3 * q + 1], ni[3 * q + 2], S, s.pt[q]);
+        const float Sq = s.pt[q] ? (S ? S[q] : local_S(p, s, ni, i, j, k)) : NAN;
+        fprintf(f, "%d,%d,%d,%g,%g,%g,%g,%d\n", i, j, k, ni[3 * q], ni[3 * q + 1], ni[3 * q + 2], Sq, s.pt[q]);
       }
   fclose(f);
   printf("  Snapshot -> %s\n", fname);
@@ -884,7 +885,7 @@ int run_modes(Params &p, Setup &s) {
   ex.pear = s.pear;
   ex.sph = s.sph;
   ex.cyl = s.cyl;
-  std::vector<float> host(s.ni.size());
+  std::vector<float> host(s.ni.size()), localS(s.ni.size() / 3);
   const std::string mode = base_mode(p.evol);
   FILE *po = fopen("po.dat", "a");
   if (!po) return fail(MCL_ERR_IO, "cannot write po.dat");
@@ -905,8 +906,9 @@ int run_modes(Params &p, Setup &s) {
       BlockResult r;
       if ((rc = measure_block(e, p, s, ex, host, r))) break;
       if ((rc = mcl_download_directors(e, 0, host.data()))) break;
+      if ((rc = mcl_local_order(e, 0, localS.data()))) break;
       snprintf(fname, sizeof fname, "director_field_%ld.csv", snapshot_index(p.T, snapS));
-      if ((rc = print_n(fname, p, s, host.data()))) break;
+      if ((rc = print_n(fname, p, s, host.data(), localS.data()))) break;
       fprintf(po, "%g %g %g %g %g", p.T, r.S1, r.S2 - r.S1 * r.S1, r.E, r.E2 - r.E * r.E);
       ex.values(po, p.MCS);
       fflush(po);
@@ -930,8 +932,9 @@ int run_modes(Params &p, Setup &s) {
       BlockResult r;
       if ((rc = measure_block(e, p, s, ex, host, r))) break;
       if ((rc = mcl_download_directors(e, 0, host.data()))) break;
+      if ((rc = mcl_local_order(e, 0, localS.data()))) break;
       snprintf(fname, sizeof fname, "director_field_%d.csv", ii);
-      if ((rc = print_n(fname, p, s, host.data()))) break;
+      if ((rc = print_n(fname, p, s, host.data(), localS.data()))) break;
       fprintf(po, "%d %g %g %g %g", ii, r.S1, r.S2 - r.S1 * r.S1, r.E, r.E2 - r.E * r.E);
       ex.values(po, p.MCS);
       fflush(po);
@@ -953,8 +956,9 @@ int run_modes(Params &p, Setup &s) {
       BlockResult r;
       if ((rc = measure_block(e, p, s, ex, host, r))) break;
       if ((rc = mcl_download_directors(e, 0, host.data()))) break;
+      if ((rc = mcl_local_order(e, 0, localS.data()))) break;
       snprintf(fname, sizeof fname, "director_field_%ld.csv", snapshot_index(p.elecE, snapS));
-      if ((rc = print_n(fname, p, s, host.data()))) break;
+      if ((rc = print_n(fname, p, s, host.data(), localS.data()))) break;
       fprintf(po, "%g %g %g %g %g", p.elecE, r.S1, r.S2 - r.S1 * r.S1, r.E, r.E2 - r.E * r.E);
       ex.values(po, p.MCS);
       fflush(po);

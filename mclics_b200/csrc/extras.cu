@@ -8,6 +8,7 @@
 #include <cmath>
 
 #include "common.cuh"
+#include "eigen3.cuh"
 #include "engine.h"
 #include "launch.h"
 #include "physics.cuh"
@@ -114,6 +115,50 @@ __global__ void k_extras_reduce(const double *__restrict__ partials, int n_block
   out[k] = v;
 }
 
+// Local order parameter of every site (src/parameter_order.cpp:75-127): Q over the site and its present
+// neighbours, accumulated in FP32 in the reference's visiting order (-x, -y, -z, the site, +z, +y, +x), divided by
+// 2 x points, then the largest eigenvalue (FP64 Jacobi). NaN on empty sites. out: nx ny nz floats, reference order.
+template <int GEO>
+__global__ void __launch_bounds__(kThreads) k_local_order(RepDesc R, const float *__restrict__ dir,
+                                                          const uint8_t *__restrict__ pt,
+                                                          const float *__restrict__ nrm, float *__restrict__ out) {
+  const long long N = (long long)R.nx * R.ny * R.nz;
+  const long long q = (long long)blockIdx.x * kThreads + threadIdx.x;
+  if (q >= N) return;
+  const unsigned qq = (unsigned)q, row = qq / (unsigned)R.nx;
+  const int x = (int)(qq - row * (unsigned)R.nx);
+  const int z = (int)(row / (unsigned)R.ny), y = (int)(row - (unsigned)z * (unsigned)R.ny);
+  Vec3 a, nb[6], s;
+  float w[6];
+  int sid;
+  if (!gather_site_rows<GEO>(R, dir, pt, nrm, x, y, z, a, nb, w, sid, s)) {
+    out[q] = __int_as_float(0x7fc00000);
+    return;
+  }
+  float Q[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  int points = 0;
+  const int order[7] = {1, 3, 5, -1, 4, 2, 0};  // -1: the site itself
+#pragma unroll
+  for (int o = 0; o < 7; o++) {
+    const int d = order[o];
+    if (d >= 0 && w[d] == 0.f) continue;
+    const Vec3 v = d < 0 ? a : nb[d];
+    const float c[3] = {v.x, v.y, v.z};
+#pragma unroll
+    for (int l = 0; l < 3; l++) {
+#pragma unroll
+      for (int m = 0; m <= l; m++) Q[3 * m + l] = (float)((double)Q[3 * m + l] + 3.0 * (double)__fmul_rn(c[l], c[m]));
+      Q[4 * l] = __fadd_rn(Q[4 * l], -1.f);
+    }
+    points++;
+  }
+  const double den = 2.0 * points;
+  double qd[6] = {(float)(Q[0] / den), (float)(Q[1] / den), (float)(Q[2] / den),
+                  (float)(Q[4] / den), (float)(Q[5] / den), (float)(Q[8] / den)};
+  double v3[3];
+  out[q] = (float)largest_eigen3(qd, v3);
+}
+
 }  // namespace mcl
 
 using namespace mcl;
@@ -162,5 +207,31 @@ extern "C" int mcl_measure_extras(mcl_engine *e, int replica, const double direc
   out->Pr_sph = v[10] > 0 ? v[9] / v[10] : 0.0;
   out->Sr_cyl = v[13] > 0 ? v[11] / v[13] : 0.0;
   out->Pr_cyl = v[13] > 0 ? v[12] / v[13] : 0.0;
+  return MCL_OK;
+}
+
+extern "C" int mcl_local_order(mcl_engine *e, int replica, float *S) {
+  if (!e || !S) return fail(MCL_ERR_ARG, "mcl_local_order: null argument");
+  if (replica < 0 || replica >= e->n_rep) return fail(MCL_ERR_ARG, "replica %d outside 0..%d", replica, e->n_rep - 1);
+  if (!e->geometry_set) return fail(MCL_ERR_STATE, "custom geometry: call mcl_set_geometry first");
+  const RepDesc &D = e->desc[replica];
+  const long long N = (long long)D.nx * D.ny * D.nz;
+  const int n_blocks = (int)((N + kThreads - 1) / kThreads);
+  const LaunchCtx c = e->ctx();
+  float *out = e->d_stage;  // max_sites x 3 floats, free between uploads and downloads
+  switch (e->geo) {
+    case GEO_BULK:
+      k_local_order<GEO_BULK><<<n_blocks, kThreads, 0, c.stream>>>(D, c.dir, c.pt, c.nrm, out);
+      break;
+    case GEO_SLAB:
+      k_local_order<GEO_SLAB><<<n_blocks, kThreads, 0, c.stream>>>(D, c.dir, c.pt, c.nrm, out);
+      break;
+    default:
+      k_local_order<GEO_PT><<<n_blocks, kThreads, 0, c.stream>>>(D, c.dir, c.pt, c.nrm, out);
+  }
+  CKX(cudaGetLastError());
+  e->launches++;
+  CKX(cudaMemcpyAsync(S, out, (size_t)N * sizeof(float), cudaMemcpyDeviceToHost, c.stream));
+  CKX(cudaStreamSynchronize(c.stream));
   return MCL_OK;
 }

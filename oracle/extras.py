@@ -78,3 +78,33 @@ def extras(ni, pt, shape, periodic, director):
         out["Sr_" + name] = s_ / n_ if n_ else 0.0
         out["Pr_" + name] = p_ / n_ if n_ else 0.0
     return out
+
+
+def local_S(ni, pt, shape, periodic, i, j, k):
+    """lattice_order_parameter (src/parameter_order.cpp:75-127): Q over the site and its present neighbours in the
+    reference's visiting order, float accumulation, largest eigenvalue in double."""
+    Nx, Ny, Nz = shape
+    ni = np.asarray(ni, np.float32).reshape(-1, 3)
+    f = np.float32
+    Q = np.zeros(9, np.float32)
+    points = 0
+    for di in (-1, 0, 1):
+        for dj in (-1, 0, 1):
+            for dk in (-1, 0, 1):
+                if abs(di) + abs(dj) + abs(dk) > 1:
+                    continue
+                ii, jj, kk = _nb(i + di, Nx, periodic[0]), _nb(j + dj, Ny, periodic[1]), _nb(k + dk, Nz, periodic[2])
+                if ii is None or jj is None or kk is None:
+                    continue
+                q = ii + Nx * (jj + Ny * kk)
+                if not pt[q]:
+                    continue
+                for l in range(3):
+                    for m in range(l + 1):
+                        Q[3 * m + l] = f(float(Q[3 * m + l]) + 3.0 * float(f(ni[q][l] * ni[q][m])))
+                    Q[4 * l] = f(Q[4 * l] - f(1))
+                points += 1
+    den = 2.0 * points
+    q = [float(f(float(Q[c]) / den)) for c in (0, 1, 2, 4, 5, 8)]
+    m = np.array([[q[0], q[1], q[2]], [q[1], q[3], q[4]], [q[2], q[4], q[5]]])
+    return float(np.linalg.eigvalsh(m)[-1])

@@ -66,3 +66,32 @@ def test_extras_match_reference_formulas(name, geo, per, shape, kind):
     if kind == "hedgehog":
         assert got["Sr_sph"] > 0.5  # radial; the polar sign is scrambled by the flip moves
     e.close()
+
+
+@pytest.mark.parametrize("geo,per,shape", [("bulk", (1, 1, 1), (6, 4, 4)), ("slab", (0, 1, 0), (5, 6, 5)),
+                                           ("sphere", (0, 0, 0), (8, 8, 8))])
+def test_local_order_matches_reference_formula(geo, per, shape):
+    nx, ny, nz = shape
+    n = nx * ny * nz
+    surfaces = [("homeotropic", 1.0, 0, 0)] * (2 if geo == "slab" else 1 if geo == "sphere" else 0)
+    e = M.Engine(M.Model("ll", surfaces=surfaces), [M.Replica(nx, ny, nz, geo, per, T=0.8, seed=5)])
+    e.upload(0, dirs(n, 11, (0.2, 0.1, 0.8)).reshape(-1))
+    e.sweeps(3)
+    cur = e.download(0).reshape(-1, 3)
+    S = e.local_order(0)
+    periodic = [bool(p) for p in per]
+    if geo == "sphere":
+        i, j, k = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+        H = np.float32(nz // 2)
+        r = np.sqrt(((i - np.float32(nx // 2)) ** 2 + (j - np.float32(ny // 2)) ** 2 + (k - H) ** 2).astype(np.float32))
+        pt = np.where(r < H - 1, 1, np.where(r < H + 1, 2, 0)).transpose(2, 1, 0).reshape(-1)
+    else:
+        pt = np.ones(n, int)
+    for q in range(n):
+        if not pt[q]:
+            assert np.isnan(S[q])
+            continue
+        i, j, k = q % nx, (q // nx) % ny, q // (nx * ny)
+        ref = X.local_S(cur, pt, shape, periodic, i, j, k)
+        assert abs(S[q] - ref) <= 1e-6 + 1e-6 * abs(ref), (q, S[q], ref)
+    e.close()
