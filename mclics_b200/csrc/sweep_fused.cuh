@@ -238,6 +238,43 @@ __device__ __forceinline__ TaskSlot make_slot(int q) {
   return s;
 }
 
+// Four cells of one half-row chunk, all three components (16-byte stores when the chunk is inside the lattice;
+// `room` = nx - x of the chunk's first site, so element e exists when 2 e < room).
+__device__ __forceinline__ void write_chunk(float *dst, long long cs, const float4 (&v)[3], bool full, int room) {
+  if (full) {
+#pragma unroll
+    for (int q = 0; q < 3; q++) *reinterpret_cast<float4 *>(dst + q * cs) = v[q];
+  } else {
+#pragma unroll
+    for (int e = 0; e < 4; e++)
+      if (2 * e < room)
+#pragma unroll
+        for (int q = 0; q < 3; q++) dst[q * cs + e] = f4get(v[q], e);
+  }
+}
+
+// Ghost copies of an edge chunk: along a periodic y the whole chunk again at rows y + ny (y < 2) and y - ny
+// (y >= ny - 2); along a periodic x, on each of those rows, x + nx for x < 2 (half index nx / 2) and x - nx for
+// x >= nx - 2 (half index -1). row0: the chunk's own half-row at half index 0.
+static __device__ __noinline__ void write_ghosts(float *row0, long long cs, int px, float4 v0, float4 v1, float4 v2,
+                                                 bool full, int room, int jl, int nx, int ny, int y, bool perx,
+                                                 bool pery) {
+  const float4 v[3] = {v0, v1, v2};
+  for (int iy = 0; iy < 3; iy++) {
+    if (iy == 1 && !(pery && y < 2)) continue;
+    if (iy == 2 && !(pery && y >= ny - 2)) continue;
+    float *rowp = row0 + (long long)(iy == 0 ? 0 : (iy == 1 ? ny : -ny)) * px;
+    if (iy > 0) write_chunk(rowp + jl, cs, v, full, room);
+    if (perx) {
+      if (jl == 0)
+        for (int q = 0; q < 3; q++) rowp[q * cs + (nx >> 1)] = v[q].x;
+      const int el = (nx >> 1) - 1 - jl;
+      if (el >= 0 && el < 4)
+        for (int q = 0; q < 3; q++) rowp[q * cs - 1] = f4get(v[q], el);
+    }
+  }
+}
+
 template <int POT, int GEO, bool FLIP, bool PXY, bool CHIRAL, bool FIELD, int TY, int NT>
 __global__ void __launch_bounds__(NT, NT <= 256 ? 2 : 1) k_sweep_fused(ModelDev m, FusedArgs a) {
   constexpr int PF = Win<TY>::PF, SLOT = Win<TY>::SLOT;
@@ -417,7 +454,6 @@ __global__ void __launch_bounds__(NT, NT <= 256 ? 2 : 1) k_sweep_fused(ModelDev 
       const int jl = j0 + 4 * w_q4;  // first half-row index of the chunk
       const int xfirst = 2 * jl + h;
       if (y < ny && xfirst < nx) {
-        const long long pbase = R.off + (long long)zw * R.py * R.px;
         int sid = -1;
         float sz = 0.f;
         if (GEO == GEO_SLAB) sid = slab_surface(zw, nz, sz);
@@ -426,35 +462,15 @@ __global__ void __launch_bounds__(NT, NT <= 256 ? 2 : 1) k_sweep_fused(ModelDev 
 #pragma unroll
         for (int q = 0; q < 3; q++) v[q] = *reinterpret_cast<const float4 *>(cw + q * PF + cell);
         const bool full = xfirst + 6 < nx;
-        // the row itself, then its ghost copies along a periodic y (y + ny for y < 2, y - ny for y >= ny - 2)
-        const bool g1 = c.pery && y < 2, g2 = c.pery && y >= ny - 2;
-#pragma unroll
-        for (int iy = 0; iy < 3; iy++) {
-          if ((iy == 1 && !g1) || (iy == 2 && !g2)) continue;
-          const int yy = iy == 0 ? y : (iy == 1 ? y + ny : y - ny);
-          float *rowp = a.out + pbase + (long long)(yy + GY) * R.px + h * R.hp + GH;  // half-row, j = 0
-          float *dst = rowp + jl;
-          if (full) {
-#pragma unroll
-            for (int q = 0; q < 3; q++) *reinterpret_cast<float4 *>(dst + q * R.comp) = v[q];
-          } else {
-#pragma unroll
-            for (int e = 0; e < 4; e++)
-              if (xfirst + 2 * e < nx)
-#pragma unroll
-                for (int q = 0; q < 3; q++) dst[q * R.comp + e] = f4get(v[q], e);
-          }
-          if (c.perx) {  // ghost columns: x + nx for x < 2 (half index nx/2), x - nx for x >= nx - 2 (index -1)
-            if (jl == 0)
-#pragma unroll
-              for (int q = 0; q < 3; q++) rowp[q * R.comp + (nx >> 1)] = v[q].x;
-            const int el = (nx >> 1) - 1 - jl;  // element holding half index nx/2 - 1 (nx is even when periodic)
-            if (el >= 0 && el < 4)
-#pragma unroll
-              for (int q = 0; q < 3; q++)
-                rowp[q * R.comp - 1] = el == 0 ? v[q].x : (el == 1 ? v[q].y : (el == 2 ? v[q].z : v[q].w));
-          }
-        }
+        // half-row (plane zw, row y, parity h) at half index 0, component 0
+        float *row0 = a.out + R.off + ((long long)zw * R.py + (y + GY)) * R.px + h * R.hp + GH;
+        const long long cs = R.comp;
+        write_chunk(row0 + jl, cs, v, full, nx - xfirst);
+        // ghost copies (edge chunks only): rows y +- ny along a periodic y, columns along a periodic x
+        const int el = (nx >> 1) - 1 - jl;  // element holding half index nx/2 - 1 (nx is even when periodic)
+        const bool gx = c.perx && (jl == 0 || (el >= 0 && el < 4));
+        const bool gy = c.pery && (y < 2 || y >= ny - 2);
+        if (gx || gy) write_ghosts(row0, cs, R.px, v[0], v[1], v[2], full, nx - xfirst, jl, nx, ny, y, c.perx, c.pery);
         if (measure) {
           float f[kPartials];
 #pragma unroll
