@@ -234,6 +234,10 @@ int mcl_extract_samples(mcl_engine *e, int replica, long long n, unsigned long l
 /* The tensor-core MLP on n feature rows (device, n x 8 floats as above) -> d_out n x 4 raw outputs (before the
  * normalisation of mu and the softplus of kappa). Synchronises `stream`. */
 int mcl_mlp_forward(const mcl_mlp *mlp, const float *d_features, long long n, float *d_out, void *stream);
+/* The same on Blackwell's tcgen05 tensor cores (operands in shared memory, accumulators in tensor memory, 256 rows
+ * per CTA); identical operand rounding, FP32 sums in another order. MCL_ERR_CUDA if a tensor-core completion does
+ * not arrive within 2 s (the CTA frees its tensor memory and stops). */
+int mcl_mlp_forward_tcgen05(const mcl_mlp *mlp, const float *d_features, long long n, float *d_out, void *stream);
 
 /* Training on the GPU: loss = -mean log(4 pi q(n | features)) over samples (maximum likelihood of the site's
  * conditional distribution), Adam (beta 0.9 / 0.999, eps 1e-8) on FP32 master weights, BF16-rounded weights in

@@ -106,6 +106,7 @@ def lib():
             "mcl_set_adaptation": [vp, i],
             "mcl_extract_samples": [vp, i, ctypes.c_longlong, ctypes.c_ulonglong, vp, vp],
             "mcl_mlp_forward": [vp, vp, ctypes.c_longlong, vp, vp],
+            "mcl_mlp_forward_tcgen05": [vp, vp, ctypes.c_longlong, vp, vp],
             "mcl_trainer_create": [vp, ctypes.c_longlong, f, P(vp)],
             "mcl_trainer_gradient": [vp, vp, vp, ctypes.c_longlong, vp, P(ctypes.c_double)],
             "mcl_trainer_step": [vp, vp, vp, ctypes.c_longlong, f, P(ctypes.c_double)],
@@ -363,11 +364,12 @@ def mlp_params(params):
     return p
 
 
-def mlp_forward(params, features_ptr, n, out_ptr, stream=0):
-    """Raw network outputs (n x 4) of the tensor-core MLP for n device feature rows (n x 8)."""
+def mlp_forward(params, features_ptr, n, out_ptr, stream=0, tcgen05=False):
+    """Raw network outputs (n x 4) of the tensor-core MLP for n device feature rows (n x 8): mma.sync warps, or
+    with tcgen05=True the fifth-generation tensor cores."""
     p = mlp_params(params)
-    check(lib().mcl_mlp_forward(p.ctypes.data, ctypes.c_void_p(features_ptr), n, ctypes.c_void_p(out_ptr),
-                                ctypes.c_void_p(stream or 0)))
+    fn = lib().mcl_mlp_forward_tcgen05 if tcgen05 else lib().mcl_mlp_forward
+    check(fn(p.ctypes.data, ctypes.c_void_p(features_ptr), n, ctypes.c_void_p(out_ptr), ctypes.c_void_p(stream or 0)))
 
 
 class Trainer:

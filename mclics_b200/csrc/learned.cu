@@ -31,6 +31,7 @@
 #include "common.cuh"
 #include "engine.h"
 #include "launch.h"
+#include "mlp_tc.cuh"
 #include "physics.cuh"
 #include "site_access.cuh"
 
@@ -232,6 +233,128 @@ __device__ __forceinline__ void warp_mlp(const MlpDev &S, __nv_bfloat16 (*As)[24
   o[2] = ov.z;
   o[3] = ov.w;
   __syncwarp();
+}
+
+// ---- the same network on tcgen05 (mlp_tc.cuh): a CTA of 256 threads, one row (site) per thread ---------------
+// Bias + SiLU of 32 accumulator columns c0 .. c0 + 31 of this thread's row, packed to BF16 into its row of a
+// K = 64 core-matrix tile.
+__device__ __forceinline__ void tc_act_store(uint8_t *tile, int row, int c0, const float (&v)[32],
+                                             const float *__restrict__ bias) {
+#pragma unroll
+  for (int ch = 0; ch < 4; ch++) {
+    uint4 p;
+    uint32_t *pp = reinterpret_cast<uint32_t *>(&p);
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const int c = 8 * ch + 2 * i;
+      pp[i] = silu2h(v[c] + bias[c0 + c], v[c + 1] + bias[c0 + c + 1]);
+    }
+    *reinterpret_cast<uint4 *>(tile + core_off(row, c0 + 8 * ch, 64)) = p;
+  }
+}
+
+// All 256 threads call it with their row's features; false (CTA-uniform) after a tensor-core timeout, in which case
+// the caller frees the tensor memory (tc_teardown) and stops.
+__device__ __forceinline__ bool cta_mlp_tc(TcSmem &S, unsigned &phase, long long timeout_ns, const float (&f)[kIn],
+                                           float (&o)[kOut]) {
+  const int tid = threadIdx.x, t = tid >> 7, row = tid & 127;
+  uint8_t *a1 = S.a1 + t * kTcA1;
+  uint4 lo;
+  lo.x = pack2(f[0], f[1]);
+  lo.y = pack2(f[2], f[3]);
+  lo.z = pack2(f[4], f[5]);
+  lo.w = pack2(f[6], 0.f);
+  *reinterpret_cast<uint4 *>(a1 + core_off(row, 0, 16)) = lo;
+  *reinterpret_cast<uint4 *>(a1 + core_off(row, 8, 16)) = make_uint4(0u, 0u, 0u, 0u);
+  constexpr uint32_t id64 = tc_idesc(128, 64), id16 = tc_idesc(128, 16);
+  if (!tc_stage(S, phase, timeout_ns, [&] {
+        for (int tt = 0; tt < 2; tt++)
+          tc_mma(S.tmem + tt * 64, tc_desc(S.a1 + tt * kTcA1, 128, 256), tc_desc(S.w1, 128, 256), id64, 0);
+      }))
+    return false;
+  const uint32_t tcol = S.tmem + ((uint32_t)(32 * ((tid >> 5) & 3)) << 16) + t * 64;
+  uint8_t *a2 = S.a2 + t * kTcA2;
+#pragma unroll
+  for (int hf = 0; hf < 2; hf++) {
+    float v[32];
+    tc_ld32(tcol + 32 * hf, v);
+    tc_act_store(a2, row, 32 * hf, v, S.b1);
+  }
+  if (!tc_stage(S, phase, timeout_ns, [&] {
+        for (int tt = 0; tt < 2; tt++)
+          for (int ks = 0; ks < 4; ks++)
+            tc_mma(S.tmem + tt * 64, tc_desc(S.a2 + tt * kTcA2 + ks * 256, 128, 1024),
+                   tc_desc(S.w2 + ks * 256, 128, 1024), id64, ks > 0);
+      }))
+    return false;
+#pragma unroll
+  for (int hf = 0; hf < 2; hf++) {  // layer 2 has completed: its input tile may be overwritten with h2
+    float v[32];
+    tc_ld32(tcol + 32 * hf, v);
+    tc_act_store(a2, row, 32 * hf, v, S.b2);
+  }
+  if (!tc_stage(S, phase, timeout_ns, [&] {
+        for (int tt = 0; tt < 2; tt++)
+          for (int ks = 0; ks < 4; ks++)
+            tc_mma(S.tmem + tt * 64, tc_desc(S.a2 + tt * kTcA2 + ks * 256, 128, 1024),
+                   tc_desc(S.w3 + ks * 256, 128, 1024), id16, ks > 0);
+      }))
+    return false;
+  float v4[4];
+  tc_ld4(tcol, v4);
+#pragma unroll
+  for (int k = 0; k < kOut; k++) o[k] = v4[k] + S.b3[k];
+  return true;
+}
+
+// Network outputs of feature rows on tcgen05 (the same outputs as k_mlp_forward).
+__global__ void __launch_bounds__(kTcRows) k_mlp_forward_tc(const MlpTC *__restrict__ w,
+                                                            const float *__restrict__ feat, long long n,
+                                                            float *__restrict__ out, unsigned *__restrict__ err,
+                                                            long long timeout_ns) {
+  extern __shared__ __align__(128) unsigned char tc_dyn[];
+  TcSmem &S = *reinterpret_cast<TcSmem *>(((uintptr_t)tc_dyn + 127) & ~(uintptr_t)127);
+  tc_setup(S, w);
+  unsigned phase = 0;
+  for (long long base = (long long)blockIdx.x * kTcRows; base < n; base += (long long)gridDim.x * kTcRows) {
+    const long long i = base + threadIdx.x;
+    float f[kIn];
+#pragma unroll
+    for (int k = 0; k < kIn; k++) f[k] = i < n ? feat[i * kFeat + k] : 0.f;
+    float o[kOut];
+    if (!cta_mlp_tc(S, phase, timeout_ns, f, o)) {
+      if (threadIdx.x == 0) atomicOr(err, 1u);
+      break;
+    }
+    if (i < n)
+#pragma unroll
+      for (int k = 0; k < kOut; k++) out[i * kOut + k] = o[k];
+  }
+  tc_teardown(S);
+}
+
+static void to_tc_layout(const mcl_mlp &p, MlpTC &d) {
+  memset(&d, 0, sizeof d);
+  const float *f = reinterpret_cast<const float *>(&p);
+  for (int n = 0; n < kH; n++) {
+    for (int k = 0; k < kIn; k++) {
+      const uint16_t b = bf16_bits(0.5f * f[oW1 + n * kIn + k]);
+      memcpy(d.w1 + core_off(n, k, 16), &b, 2);
+    }
+    for (int k = 0; k < kH; k++) {
+      const uint16_t b = bf16_bits(0.5f * f[oW2 + n * kH + k]);
+      memcpy(d.w2 + core_off(n, k, 64), &b, 2);
+    }
+    d.b1[n] = 0.5f * f[oB1 + n];
+    d.b2[n] = 0.5f * f[oB2 + n];
+  }
+  for (int n = 0; n < kOut; n++) {
+    for (int k = 0; k < kH; k++) {
+      const uint16_t b = bf16_bits(f[oW3 + n * kH + k]);
+      memcpy(d.w3 + core_off(n, k, 64), &b, 2);
+    }
+    d.b3[n] = f[oB3 + n];
+  }
 }
 
 struct Head {
@@ -796,6 +919,40 @@ int mcl_mlp_forward(const mcl_mlp *mlp, const float *d_features, long long n, fl
   if (err == cudaSuccess) err = cudaStreamSynchronize(st);
   cudaFree(d);
   if (err != cudaSuccess) return cuda_fail(err, "mcl_mlp_forward");
+  return MCL_OK;
+}
+
+int mcl_mlp_forward_tcgen05(const mcl_mlp *mlp, const float *d_features, long long n, float *d_out, void *stream) {
+  if (!mlp || n < 0 || (n > 0 && (!d_features || !d_out)))
+    return fail(MCL_ERR_ARG, "mcl_mlp_forward_tcgen05: bad arguments");
+  if (n == 0) return MCL_OK;
+  MlpTC h;
+  to_tc_layout(*mlp, h);
+  MlpTC *d = nullptr;
+  unsigned *err = nullptr;
+  CKL(cudaMalloc(&d, sizeof h));
+  cudaError_t e2 = cudaMalloc(&err, sizeof(unsigned));
+  if (e2 != cudaSuccess) {
+    cudaFree(d);
+    return cuda_fail(e2, "cudaMalloc");
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t smem = sizeof(TcSmem) + 128;
+  cudaError_t e = cudaMemcpyAsync(d, &h, sizeof h, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(unsigned), st);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mlp_forward_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) {
+    const long long blocks = std::min<long long>((n + kTcRows - 1) / kTcRows, 148ll * 2);
+    k_mlp_forward_tc<<<(unsigned)blocks, kTcRows, smem, st>>>(d, d_features, n, d_out, err, 2000000000ll);
+    e = cudaGetLastError();
+  }
+  unsigned flag = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&flag, err, sizeof flag, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(d);
+  cudaFree(err);
+  if (e != cudaSuccess) return cuda_fail(e, "mcl_mlp_forward_tcgen05");
+  if (flag) return fail(MCL_ERR_CUDA, "mcl_mlp_forward_tcgen05: a tensor-core commit did not arrive in time");
   return MCL_OK;
 }
 

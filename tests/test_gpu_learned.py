@@ -63,6 +63,27 @@ def test_mlp_forward_matches_oracle():
     assert err.mean() < 2e-3, err.mean()
 
 
+def test_tcgen05_forward_matches_mma_sync_and_oracle():
+    rng = np.random.default_rng(8)
+    n = 5000  # 19 full chunks of 256 rows and a ragged one
+    x = np.zeros((n, 8), np.float32)
+    x[:, :6] = rng.uniform(-0.5, 1.0, (n, 6))
+    x[:, 6] = rng.uniform(0.2, 1.3, n)
+    x[:, 7] = 1
+    p = perturbed_params(6)
+    feat = torch.from_numpy(x).cuda()
+    out_tc = torch.full((n, 4), float("nan"), dtype=torch.float32, device="cuda")
+    out_mma = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+    M.mlp_forward(p, feat.data_ptr(), n, out_tc.data_ptr(), tcgen05=True)
+    M.mlp_forward(p, feat.data_ptr(), n, out_mma.data_ptr())
+    a, b = out_tc.cpu().numpy().astype(np.float64), out_mma.cpu().numpy().astype(np.float64)
+    assert np.isfinite(a).all()
+    ref, _ = L.forward(p.astype(np.float64), x[:, :7].astype(np.float64))
+    # same BF16 operands and FP32 accumulation, sums in another order
+    assert np.abs(a - b).max() < 3e-2 and np.abs(a - b).mean() < 1e-3, (np.abs(a - b).max(), np.abs(a - b).mean())
+    assert np.abs(a - ref).max() < 3e-2 and np.abs(a - ref).mean() < 2e-3
+
+
 def test_extracted_features_match_oracle():
     nx = 10
     e = engine_ll(nx, 0.8, 5)
