@@ -119,6 +119,12 @@ static int ensure_series(mcl_engine *e, int rows) {
   return MCL_OK;
 }
 
+// Error words of the fused sweep (TMA waits) and the learned sweep (tensor-core waits); synchronises.
+static int kernel_errors(mcl_engine *e) {
+  const int rc = fused_check_error(e);
+  return rc ? rc : learned_check_error(e);
+}
+
 // Captured sweep graphs hold kernel arguments (work items, buffers, series, test hooks): drop them whenever one of
 // those changes.
 static void drop_graphs(mcl_engine *e) {
@@ -396,6 +402,8 @@ int mcl_destroy(mcl_engine *e) {
   cudaFree(e->d_dir[0]);
   cudaFree(e->d_dir[1]);
   cudaFree(e->d_mlp);
+  cudaFree(e->d_mlp_tc);
+  cudaFree(e->d_lerr);
   cudaFree(e->d_xpart);
   cudaFree(e->d_pt);
   cudaFree(e->d_nrm);
@@ -479,7 +487,7 @@ int mcl_download_directors(mcl_engine *e, int replica, float *ni) {
   CK(launch_pack(e->ctx(), replica, D, e->d_stage));
   CK(cudaMemcpyAsync(ni, e->d_stage, N * 3 * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
   CK(cudaStreamSynchronize(e->stream));
-  return fused_check_error(e);
+  return kernel_errors(e);
 }
 
 static int set_state_field(mcl_engine *e, int replica, size_t offset, float v) {
@@ -573,7 +581,8 @@ int mcl_sweeps(mcl_engine *e, int n, int measure) {
       LaunchCtx c = e->ctx();
       if (ev0) CK(cudaEventRecord(ev0, e->stream));
       if (e->d_mlp) {  // observables fused into the two colour kernels, finalised over the same block table
-        CK(launch_sweep_learned(c, e->geo, e->half, e->d_mlp, e->kappa_max, measure ? 1 : 0, e->d_partials));
+        const LearnedMlp lm{e->d_mlp, e->d_mlp_tc, e->d_lerr, e->mlp_tc};
+        CK(launch_sweep_learned(c, e->geo, e->half, lm, e->kappa_max, measure ? 1 : 0, e->d_partials));
         e->launches += 2;
         if (ev1) CK(cudaEventRecord(ev1, e->stream));
         CK(launch_finalize(c, e->half, e->d_partials, measure ? 1 : 0, e->d_series, e->d_series_len, e->d_done));
@@ -663,7 +672,7 @@ int mcl_read_series(mcl_engine *e, int replica, int first, int count, mcl_observ
                        (size_t)e->n_rep * sizeof(ObsRecord), sizeof(ObsRecord), count, cudaMemcpyDeviceToHost,
                        e->stream));
   CK(cudaStreamSynchronize(e->stream));
-  if ((rc = fused_check_error(e))) return rc;
+  if ((rc = kernel_errors(e))) return rc;
   for (int i = 0; i < count; i++) to_public(rows[i], out + i);
   return MCL_OK;
 }
@@ -686,7 +695,7 @@ int mcl_measure(mcl_engine *e, int replica, mcl_observables *out) {
   ObsRecord o;
   CK(cudaMemcpyAsync(&o, e->d_probe + replica, sizeof o, cudaMemcpyDeviceToHost, e->stream));
   CK(cudaStreamSynchronize(e->stream));
-  if ((rc = fused_check_error(e))) return rc;
+  if ((rc = kernel_errors(e))) return rc;
   to_public(o, out);
   return MCL_OK;
 }
@@ -695,7 +704,7 @@ int mcl_synchronize(mcl_engine *e) {
   if (!e) return fail(MCL_ERR_ARG, "null engine");
   CK(cudaStreamSynchronize(e->stream));
   CK(cudaGetLastError());
-  return fused_check_error(e);
+  return kernel_errors(e);
 }
 
 int mcl_debug_wait_limit(mcl_engine *e, long long timeout_ns, int withhold_first_load) {

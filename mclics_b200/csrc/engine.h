@@ -17,6 +17,8 @@ int cuda_fail(cudaError_t err, const char *what);
 
 struct FusedPlan;  // fused tiled sweep (sweep_fused.cu)
 struct MlpDev;     // learned proposal weights in device layout (learned.cu)
+struct MlpTC;      // the same in the tcgen05 layout (mlp_tc.cuh)
+int learned_check_error(mcl_engine *e);
 
 }  // namespace mcl
 
@@ -66,6 +68,9 @@ struct mcl_engine {
   long long prof_sweeps = 0;
   long long launches = 0;      // kernels launched by this engine
   mcl::MlpDev *d_mlp = nullptr;  // learned proposal (null: plain proposal)
+  mcl::MlpTC *d_mlp_tc = nullptr;  // the same weights in the tcgen05 layout
+  unsigned *d_lerr = nullptr;      // learned-sweep error word
+  bool mlp_tc = true;              // learned sweeps run the network on tcgen05
   double *d_xpart = nullptr;   // scratch of mcl_measure_extras (allocated at its first call)
   float kappa_max = 500.f;
   bool adapt = true;           // ang_var adaptation after each sweep (the reference's behaviour)

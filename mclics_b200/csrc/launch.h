@@ -46,7 +46,14 @@ cudaError_t launch_refresh_ghosts(const LaunchCtx &c, int max_ny_nz, int max_px_
 // measure, the observables of the final state go to partials[block of `half`][kPartials] (reduce them with
 // launch_finalize over the same table).
 struct MlpDev;
-cudaError_t launch_sweep_learned(const LaunchCtx &c, int geo, const BlockTable &half, const MlpDev *mlp,
+struct MlpTC;
+struct LearnedMlp {
+  const MlpDev *warp;  // weights for the mma.sync warps
+  const MlpTC *tc;     // weights for tcgen05
+  unsigned *err;       // error word (tensor-core timeout)
+  bool use_tc;
+};
+cudaError_t launch_sweep_learned(const LaunchCtx &c, int geo, const BlockTable &half, const LearnedMlp &mlp,
                                  float kappa_max, int measure, double *partials);
 // AoS (reference layout) <-> padded SoA for one replica.
 cudaError_t launch_unpack(const LaunchCtx &c, int replica, const RepDesc &host_desc, const float *aos);

@@ -418,7 +418,13 @@ __device__ __forceinline__ Vec3 sample_proposal(const Head &h, float em1, float 
 __device__ __forceinline__ float u24(uint32_t v) { return (float)(v >> 8) * 0x1p-24f; }
 
 // ---- the learned sweep: one colour, one thread per site ----------------------------------------------------------
-template <int POT, int GEO>
+// TC: the network on tcgen05 (a CTA-wide pass over its 256 sites) instead of mma.sync warps. Dynamic shared memory:
+// TcSmem (TC) or the warp path's weights and scratch.
+constexpr size_t kWarpMlpSmem = sizeof(MlpDev) + sizeof(__nv_bfloat16) * (kThreads / 32) * 32 * 24 +
+                                sizeof(float) * (kThreads / 32) * 32 * 4 + 128;
+constexpr size_t kTcMlpSmem = sizeof(TcSmem) + 128;
+
+template <int POT, int GEO, bool TC>
 __global__ void __launch_bounds__(kThreads, 3) k_sweep_learned(ModelDev m, const RepDesc *__restrict__ reps,
                                                             RepState *__restrict__ st, float *__restrict__ dir,
                                                             const uint8_t *__restrict__ pt,
@@ -426,15 +432,30 @@ __global__ void __launch_bounds__(kThreads, 3) k_sweep_learned(ModelDev m, const
                                                             const unsigned long long *__restrict__ sweep_ctr,
                                                             int colour, const int *__restrict__ blk_rep,
                                                             const long long *__restrict__ blk_base, int n_blocks,
-                                                            const MlpDev *__restrict__ mlp, float kappa_max,
+                                                            const MlpDev *__restrict__ mlp,
+                                                            const MlpTC *__restrict__ mlp_tc,
+                                                            unsigned *__restrict__ err, float kappa_max,
                                                             int measure, double *__restrict__ partials) {
-  __shared__ __align__(16) MlpDev S;
+  extern __shared__ __align__(128) unsigned char ls_dyn[];
   __shared__ double red[kThreads / 32][kPartials];
-  __shared__ __align__(16) __nv_bfloat16 As[kThreads / 32][32][24];
-  __shared__ __align__(16) float Out[kThreads / 32][32][4];
-  for (int i = threadIdx.x; i < (int)(sizeof(MlpDev) / 16); i += blockDim.x)
-    reinterpret_cast<uint4 *>(&S)[i] = reinterpret_cast<const uint4 *>(mlp)[i];
-  __syncthreads();
+  unsigned char *sbase = (unsigned char *)(((uintptr_t)ls_dyn + 127) & ~(uintptr_t)127);
+  MlpDev *S = nullptr;
+  __nv_bfloat16(*As)[32][24] = nullptr;
+  float(*Out)[32][4] = nullptr;
+  TcSmem *T = nullptr;
+  unsigned phase = 0;
+  if constexpr (TC) {
+    T = reinterpret_cast<TcSmem *>(sbase);
+    tc_setup(*T, mlp_tc);
+  } else {
+    S = reinterpret_cast<MlpDev *>(sbase);
+    As = reinterpret_cast<__nv_bfloat16(*)[32][24]>(sbase + sizeof(MlpDev));
+    Out = reinterpret_cast<float(*)[32][4]>(sbase + sizeof(MlpDev) +
+                                            sizeof(__nv_bfloat16) * (kThreads / 32) * 32 * 24);
+    for (int i = threadIdx.x; i < (int)(sizeof(MlpDev) / 16); i += blockDim.x)
+      reinterpret_cast<uint4 *>(S)[i] = reinterpret_cast<const uint4 *>(mlp)[i];
+    __syncthreads();
+  }
   const int warp = threadIdx.x >> 5;
   const unsigned long long sweep = *sweep_ctr;
   for (int b = blockIdx.x; b < n_blocks; b += gridDim.x) {
@@ -465,7 +486,14 @@ __global__ void __launch_bounds__(kThreads, 3) k_sweep_learned(ModelDev m, const
     float f[kIn] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     if (valid) site_features(nb, w, St.T, f);
     float o[kOut];
-    warp_mlp(S, As[warp], Out[warp], f, o);
+    if constexpr (TC) {
+      if (!cta_mlp_tc(*T, phase, 2000000000ll, f, o)) {  // CTA-uniform: stop, report, free the tensor memory
+        if (threadIdx.x == 0) atomicOr(err, 1u);
+        break;
+      }
+    } else {
+      warp_mlp(*S, As[warp], Out[warp], f, o);
+    }
     unsigned accepted = 0;
     float ob[kPartials] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     if (valid) {
@@ -529,6 +557,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_sweep_learned(ModelDev m, const
       __syncthreads();
     }
   }
+  if constexpr (TC) tc_teardown(*T);
 }
 
 // Network outputs (before the head) for feature rows, for parity tests of the tensor-core path.
@@ -778,28 +807,37 @@ __global__ void k_round(const float *__restrict__ params, float *__restrict__ wr
 }
 
 // ---- launchers -------------------------------------------------------------------------------------------------
-template <int POT>
-static void sweep_learned_pot(const LaunchCtx &c, int geo, const BlockTable &t, int colour, const MlpDev *mlp,
+template <int POT, int GEO, bool TC>
+static void sweep_learned_one(const LaunchCtx &c, const BlockTable &t, int colour, const LearnedMlp &mlp,
                               float kappa_max, int grid, int measure, double *partials) {
-  switch (geo) {
-    case GEO_BULK:
-      k_sweep_learned<POT, GEO_BULK><<<grid, kThreads, 0, c.stream>>>(c.model, c.reps, c.state, c.dir, c.pt, c.nrm,
-                                                                       c.sweep_ctr, colour, t.rep, t.base, t.n_blocks,
-                                                                       mlp, kappa_max, measure, partials);
-      break;
-    case GEO_SLAB:
-      k_sweep_learned<POT, GEO_SLAB><<<grid, kThreads, 0, c.stream>>>(c.model, c.reps, c.state, c.dir, c.pt, c.nrm,
-                                                                       c.sweep_ctr, colour, t.rep, t.base, t.n_blocks,
-                                                                       mlp, kappa_max, measure, partials);
-      break;
-    default:
-      k_sweep_learned<POT, GEO_PT><<<grid, kThreads, 0, c.stream>>>(c.model, c.reps, c.state, c.dir, c.pt, c.nrm,
-                                                                     c.sweep_ctr, colour, t.rep, t.base, t.n_blocks,
-                                                                     mlp, kappa_max, measure, partials);
-  }
+  auto k = k_sweep_learned<POT, GEO, TC>;
+  const size_t smem = TC ? kTcMlpSmem : kWarpMlpSmem;
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k<<<grid, kThreads, smem, c.stream>>>(c.model, c.reps, c.state, c.dir, c.pt, c.nrm, c.sweep_ctr, colour, t.rep,
+                                        t.base, t.n_blocks, mlp.warp, mlp.tc, mlp.err, kappa_max, measure, partials);
 }
 
-cudaError_t launch_sweep_learned(const LaunchCtx &c, int geo, const BlockTable &half, const MlpDev *mlp,
+template <int POT>
+static void sweep_learned_pot(const LaunchCtx &c, int geo, const BlockTable &t, int colour, const LearnedMlp &mlp,
+                              float kappa_max, int grid, int measure, double *partials) {
+  if (mlp.use_tc) {
+    if (geo == GEO_BULK)
+      sweep_learned_one<POT, GEO_BULK, true>(c, t, colour, mlp, kappa_max, grid, measure, partials);
+    else if (geo == GEO_SLAB)
+      sweep_learned_one<POT, GEO_SLAB, true>(c, t, colour, mlp, kappa_max, grid, measure, partials);
+    else
+      sweep_learned_one<POT, GEO_PT, true>(c, t, colour, mlp, kappa_max, grid, measure, partials);
+    return;
+  }
+  if (geo == GEO_BULK)
+    sweep_learned_one<POT, GEO_BULK, false>(c, t, colour, mlp, kappa_max, grid, measure, partials);
+  else if (geo == GEO_SLAB)
+    sweep_learned_one<POT, GEO_SLAB, false>(c, t, colour, mlp, kappa_max, grid, measure, partials);
+  else
+    sweep_learned_one<POT, GEO_PT, false>(c, t, colour, mlp, kappa_max, grid, measure, partials);
+}
+
+cudaError_t launch_sweep_learned(const LaunchCtx &c, int geo, const BlockTable &half, const LearnedMlp &mlp,
                                  float kappa_max, int measure, double *partials) {
   if (half.n_blocks == 0) return cudaSuccess;
   int dev = 0, sms = 148;
@@ -845,6 +883,20 @@ static bool finite_params(const mcl_mlp *p) {
   return true;
 }
 
+namespace mcl {
+int learned_check_error(mcl_engine *e) {
+  if (!e->d_lerr) return MCL_OK;
+  unsigned v = 0;
+  CKL(cudaMemcpyAsync(&v, e->d_lerr, sizeof v, cudaMemcpyDeviceToHost, e->stream));
+  CKL(cudaStreamSynchronize(e->stream));
+  if (v) {
+    CKL(cudaMemsetAsync(e->d_lerr, 0, sizeof v, e->stream));
+    return fail(MCL_ERR_CUDA, "learned sweep: a tensor-core completion did not arrive within 2 s");
+  }
+  return MCL_OK;
+}
+}  // namespace mcl
+
 extern "C" {
 
 int mcl_set_proposal(mcl_engine *e, const mcl_mlp *mlp, float kappa_max) {
@@ -860,9 +912,20 @@ int mcl_set_proposal(mcl_engine *e, const mcl_mlp *mlp, float kappa_max) {
   if (!finite_params(mlp)) return fail(MCL_ERR_NONFINITE, "mcl_set_proposal: non-finite weight");
   MlpDev h;
   to_device_layout(*mlp, h);
+  MlpTC ht;
+  to_tc_layout(*mlp, ht);
   if (!e->d_mlp) CKL(cudaMalloc(&e->d_mlp, sizeof(MlpDev)));
+  if (!e->d_mlp_tc) CKL(cudaMalloc(&e->d_mlp_tc, sizeof(MlpTC)));
+  if (!e->d_lerr) {
+    CKL(cudaMalloc(&e->d_lerr, sizeof(unsigned)));
+    CKL(cudaMemset(e->d_lerr, 0, sizeof(unsigned)));
+  }
   CKL(cudaMemcpy(e->d_mlp, &h, sizeof h, cudaMemcpyHostToDevice));
+  CKL(cudaMemcpy(e->d_mlp_tc, &ht, sizeof ht, cudaMemcpyHostToDevice));
   e->kappa_max = kappa_max;
+  // tcgen05 unless MCL_LEARNED_MLP=mma selects the mma.sync warps (same network, same rounding points)
+  const char *path = getenv("MCL_LEARNED_MLP");
+  e->mlp_tc = !(path && strcmp(path, "mma") == 0);
   return MCL_OK;
 }
 
