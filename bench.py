@@ -270,8 +270,13 @@ def gpu_arm(args, rank, world, local_rank):
     for _ in range(args.warmup):
         eng.sweeps(1, measure=True)
     eng.synchronize()
-    # tile plan by the autotuner (state restored), then graph replay of the fused sweeps
-    tuning = eng.autotune(3)
+    # tile plan by the autotuner (state restored) or given by --plan, then graph replay of the sweeps
+    if args.plan:
+        cfg_s, _, seg_s = args.plan.partition(",")
+        eng.set_plan(int(cfg_s), int(seg_s or 0))
+        tuning = dict(eng.plan(), candidates=0)
+    else:
+        tuning = eng.autotune(3)
     eng.set_graphs(True)
     eng.sweeps(2, measure=True)  # captures the graph outside the timed region
     eng.synchronize()
@@ -376,7 +381,7 @@ def learned_compare(args):
     for arm in ("plain", "learned"):
         e = engine(7)
         e.set_stream(stream.cuda_stream)
-        e.sweeps(1000)
+        e.sweeps(args.therm_sweeps)  # ~10 tau_E at T = 1.12 (tau_E ~ 500 sweeps for the plain proposal)
         if arm == "plain":
             e.set_adaptation(False)
         else:
@@ -413,7 +418,7 @@ def learned_compare(args):
     line = {"metric": "ESS/s (tau_int of E and S), learned vs plain proposal, min over E and S at %s" % tnis,
             "value": min(per_T[tnis]["ess_ratio_E"], per_T[tnis]["ess_ratio_S"]), "unit": "ratio",
             "higher_is_better": True, "n_gpus": 1, "steps": K, "data": "synthetic", "dtype": "f32 / bf16 MLP",
-            "config": dict(cfg, start="(0,0,1) + 0.1 uniform noise, 1000 thermalisation sweeps",
+            "config": dict(cfg, start="(0,0,1) + 0.1 uniform noise, %d thermalisation sweeps" % args.therm_sweeps,
                            sweeps_per_arm=K, tau_window="Sokal, c = 5"),
             "training": {"samples": n_samples, "collect_s": t1 - t0, "train_s": t2 - t1, "steps": len(losses),
                          "loss_first": float(losses[:20].mean()), "loss_last": float(losses[-50:].mean()),
@@ -435,6 +440,10 @@ def main():
     ap.add_argument("--learned", action="store_true",
                     help="learned vs plain proposal: train the proposal network, compare ESS/s of E and S")
     ap.add_argument("--ess-sweeps", type=int, default=10000)
+    ap.add_argument("--plan", default="",
+                    help="tile configuration[,planes per z segment] instead of the autotuner (profiling runs)")
+    ap.add_argument("--therm-sweeps", type=int, default=5000,
+                    help="--learned: plain sweeps from the ordered start before both arms are measured")
     ap.add_argument("--train-samples", type=int, default=10_000_000)
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"],
                     help="c2 (default): the headline GHRL 256^3 slab; others: the remaining configurations")
@@ -497,7 +506,10 @@ def main():
     sites_total = res["all_sites"] if sharded else res["sites"] * world
     config["global_sites_per_step"] = sites_total
     tu = res["tuning"]
-    config["plan"] = {"autotuned": True, "rows_per_tile": tu["rows_per_tile"], "threads_per_cta": tu["threads_per_cta"],
+    config["plan"] = {"autotuned": not args.plan, "tile_config": tu["tile_config"],
+                      "kernel": ("two in-place colour passes per sweep" if tu["tile_config"] >= 2 else
+                                 "fused two-colour sweep (ping-pong buffers)"),
+                      "rows_per_tile": tu["rows_per_tile"], "threads_per_cta": tu["threads_per_cta"],
                       "planes_per_segment": tu["planes_per_segment"], "ctas": tu["work_items"],
                       "candidates": tu["candidates"], "cuda_graph": True}
     config["l2"] = ("inputs larger than L2 (%.0f MB of directors > 126 MB)" % (res["sites"] * 12 / 1e6)

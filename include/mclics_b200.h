@@ -180,13 +180,18 @@ int mcl_local_order(mcl_engine *e, int replica, float *S);
 /* ---- Batched sweeps: tuning and graph replay (no counterpart in the reference: it runs one lattice per process,
  * src/evolve.cu:317-440) ----------------------------------------------------------------------------------------
  * The replicas of an engine are swept together: every work item (replica, tile, z segment) of every replica is one
- * CTA of one launch. mcl_autotune times each candidate plan — tile configuration (64 x 14 sites with 256 threads
- * per CTA, or 64 x 28 with 512) and planes per z segment — for trial_sweeps measured sweeps on the engine's own
- * replicas, keeps the fastest and restores the directors, per-replica state, sweep counter and series, so the run
- * continues as if it had not been called. MCL_ERR_STATE unless the engine runs the fused sweep (bulk/slab, plain
- * proposal, no decision recording). */
+ * CTA of one launch. A plan is a tile configuration and a number of planes per z segment. Tile configurations:
+ *   0: fused sweep (both colours in one launch, ping-pong buffers), 64 x 14 sites, 256 threads per CTA;
+ *   1: fused sweep, 64 x 28 sites, 512 threads;
+ *   2: two in-place colour passes per sweep, 64 x 16 sites, 256 threads, 3 CTAs per SM;
+ *   3: colour passes, 64 x 32 sites, 512 threads;
+ *   4: colour passes, 64 x 16 sites, 256 threads, 2 CTAs per SM.
+ * Every configuration gives bit-identical directors. mcl_autotune times each candidate plan for trial_sweeps
+ * measured sweeps on the engine's own replicas, keeps the fastest and restores the directors, per-replica state,
+ * sweep counter and series, so the run continues as if it had not been called. MCL_ERR_STATE unless the engine
+ * runs the tiled sweep (bulk/slab, plain proposal, no decision recording). */
 typedef struct mcl_tuning {
-  int tile_config;        /* 0 or 1 as above */
+  int tile_config;        /* 0..4 as above */
   int rows_per_tile;
   int threads_per_cta;
   int planes_per_segment;
@@ -196,6 +201,10 @@ typedef struct mcl_tuning {
   double ms_default;      /* the plan in use before the call */
 } mcl_tuning;
 int mcl_autotune(mcl_engine *e, int trial_sweeps, mcl_tuning *out);
+/* Applies a plan (e.g. one mcl_autotune chose earlier) without timing: planes_per_segment <= 0 lets the heuristic
+ * choose. mcl_get_plan fills the plan fields of *out (tile_config .. work_items; the timing fields are 0). */
+int mcl_set_plan(mcl_engine *e, int tile_config, int planes_per_segment);
+int mcl_get_plan(mcl_engine *e, mcl_tuning *out);
 /* With enable != 0, mcl_sweeps replays a captured CUDA graph of two fused sweeps (captured at the first call, again
  * after the plan, the series buffer or the test hooks change) instead of launching kernels one by one; results are
  * identical. Profiling (mcl_profile) uses direct launches. */

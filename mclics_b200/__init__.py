@@ -103,6 +103,8 @@ def lib():
             "mcl_measure_extras": [vp, i, P(ctypes.c_double * 3), P(CExtras)],
             "mcl_local_order": [vp, i, vp],
             "mcl_set_graphs": [vp, i],
+            "mcl_set_plan": [vp, i, i],
+            "mcl_get_plan": [vp, P(CTuning)],
             "mcl_set_adaptation": [vp, i],
             "mcl_extract_samples": [vp, i, ctypes.c_longlong, ctypes.c_ulonglong, vp, vp],
             "mcl_mlp_forward": [vp, vp, ctypes.c_longlong, vp, vp],
@@ -344,6 +346,15 @@ class Engine:
         t = CTuning()
         check(lib().mcl_autotune(self._h, trial_sweeps, ctypes.byref(t)))
         return {k: getattr(t, k) for k, _ in CTuning._fields_}
+
+    def set_plan(self, tile_config, planes_per_segment=0):
+        """Applies a plan without timing it (tile configuration 0..4, planes per z segment; 0: heuristic)."""
+        check(lib().mcl_set_plan(self._h, tile_config, planes_per_segment))
+
+    def plan(self):
+        t = CTuning()
+        check(lib().mcl_get_plan(self._h, ctypes.byref(t)))
+        return {k: getattr(t, k) for k, _ in CTuning._fields_ if not k.startswith("ms_") and k != "candidates"}
 
     def set_graphs(self, on=True):
         check(lib().mcl_set_graphs(self._h, 1 if on else 0))

@@ -559,7 +559,7 @@ int mcl_sweeps(mcl_engine *e, int n, int measure) {
     }
     for (; n >= 2; n -= 2) {
       CK(cudaGraphLaunch(e->graph[m], e->stream));
-      e->launches += 4;
+      e->launches += 2 * fused_launches_per_sweep(e);
       if (measure) e->series_len += 2;
     }
   }
@@ -814,6 +814,28 @@ int mcl_autotune(mcl_engine *e, int trial_sweeps, mcl_tuning *out) {
   }
 #undef CKT
   return done(MCL_OK);
+}
+
+int mcl_set_plan(mcl_engine *e, int tile_config, int planes_per_segment) {
+  if (!e) return fail(MCL_ERR_ARG, "null engine");
+  if (!e->fused) return fail(MCL_ERR_STATE, "mcl_set_plan: the engine does not run the tiled sweep");
+  drop_graphs(e);
+  return fused_set_plan(e, tile_config, planes_per_segment);
+}
+
+int mcl_get_plan(mcl_engine *e, mcl_tuning *out) {
+  if (!e || !out) return fail(MCL_ERR_ARG, "null argument");
+  if (!e->fused) return fail(MCL_ERR_STATE, "mcl_get_plan: the engine does not run the tiled sweep");
+  int cfg = 0, ty = 0, seg = 0, items = 0;
+  const int rc = fused_get_cfg(e, &cfg, &ty, &seg, &items);
+  if (rc) return rc;
+  *out = mcl_tuning{};
+  out->tile_config = cfg;
+  out->rows_per_tile = ty;
+  out->threads_per_cta = fused_threads(cfg);
+  out->planes_per_segment = seg;
+  out->work_items = items;
+  return MCL_OK;
 }
 
 int mcl_record_decisions(mcl_engine *e, int enable) {

@@ -20,7 +20,9 @@ namespace mcl {
 int fused_check_error(mcl_engine *e);
 // Test hook: wait limit in ns (> 0 to change) and whether the first TMA load of every CTA is withheld.
 void fused_set_test_hooks(mcl_engine *e, long long timeout_ns, int skip_first_load);
-// Tile configuration of the fused sweep (0: 64 x 14 tiles, 256 threads, 2 CTAs/SM; 1: 64 x 30, 512 threads).
+// Tile configuration: 0: fused, 64 x 14 tiles, 256 threads; 1: fused, 64 x 28, 512 threads; 2: colour passes,
+// 64 x 16, 256 threads, 3 CTAs/SM; 3: colour passes, 64 x 32, 512 threads; 4: colour passes, 64 x 16, 256 threads,
+// 2 CTAs/SM.
 int fused_set_cfg(mcl_engine *e, int cfg);
 int fused_get_cfg(const mcl_engine *e, int *cfg, int *ty, int *seg, int *items);
 // Tile configuration and planes per z segment (seg <= 0: the heuristic's choice); rebuilds the work items.
@@ -28,4 +30,6 @@ int fused_set_plan(mcl_engine *e, int cfg, int seg);
 // Candidate (configuration, planes per segment) pairs for the autotuner, and the threads per CTA of a configuration.
 void fused_plan_candidates(const mcl_engine *e, std::vector<std::pair<int, int>> &out);
 int fused_threads(int cfg);
+// Kernel launches of one sweep of the current plan, finalisation included (fused: 2, colour passes: 3).
+int fused_launches_per_sweep(const mcl_engine *e);
 }  // namespace mcl

@@ -1,5 +1,6 @@
-// Fused two-colour sweep: host side (tensor maps, work items, tile configuration, launches). The kernel and its
-// description are in sweep_fused.cuh.
+// Tiled sweeps on TMA-streamed planes, host side (tensor maps, work items, tile configuration, launches): the fused
+// two-colour kernel (sweep_fused.cuh) and the in-place colour passes (sweep_pass.cuh) share the work items, the
+// per-item partials and the finalisation; the tile configuration selects the kernel.
 #include <stdlib.h>
 
 #include <algorithm>
@@ -7,11 +8,13 @@
 #include <vector>
 
 #include "fused.h"
-#include "sweep_fused.cuh"
+#include "sweep_pass.cuh"
 
 namespace mcl {
 
-static const FusedCfg kCfgs[kNumCfgs] = {{14, 256, 2}, {28, 512, 1}};
+// 0, 1: fused (7 slots of TY + 4 rows: one CTA per SM either way); 2-4: colour passes (4 slots of TY + 2 rows).
+static const FusedCfg kCfgs[kNumCfgs] = {{14, 256, 1, 0}, {28, 512, 1, 0}, {16, 256, 3, 1}, {32, 512, 1, 1},
+                                         {16, 256, 2, 1}};
 
 struct FusedPlan {
   int cfg = 0, tx = 64, ty = 14, seg = 32;
@@ -49,11 +52,12 @@ bool fused_supported(const mcl_engine *e) {
   return get_encode() != nullptr;
 }
 
-static int encode_map(CUtensorMap *map, float *base, const RepDesc &D, int ty) {
+// Box of `rows` padded rows (fused: TY + 4, colour pass: TY + 2).
+static int encode_map(CUtensorMap *map, float *base, const RepDesc &D, int rows) {
   // 5-D view of the split layout: (half-row cell, x parity, padded row, plane, component)
   cuuint64_t dims[5] = {(cuuint64_t)D.hp, 2, (cuuint64_t)D.py, (cuuint64_t)D.nz, 3};
   cuuint64_t strides[4] = {(cuuint64_t)D.hp * 4, (cuuint64_t)D.px * 4, (cuuint64_t)D.px * D.py * 4, (cuuint64_t)D.comp * 4};
-  cuuint32_t box[5] = {(cuuint32_t)HALF, 2, (cuuint32_t)(ty + 4), 1, 3};
+  cuuint32_t box[5] = {(cuuint32_t)HALF, 2, (cuuint32_t)rows, 1, 3};
   cuuint32_t es[5] = {1, 1, 1, 1, 1};
   CUresult r = get_encode()(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, base + D.off, dims, strides, box, es,
                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -69,7 +73,8 @@ static int encode_map(CUtensorMap *map, float *base, const RepDesc &D, int ty) {
   } while (0)
 
 // Tile and segment choice for configuration `cfg`: z segments sized so that the number of work items is close to
-// a multiple of the resident CTAs, with segments long enough that the four extra planes of each stay cheap.
+// a multiple of the resident CTAs, with segments long enough that the extra planes of each stay cheap (fused: four
+// loaded, two of them computed; colour pass: two loaded).
 static void choose_segments(const mcl_engine *e, FusedPlan &P, int sms) {
   const FusedCfg &C = kCfgs[P.cfg];
   P.tx = TXF;
@@ -88,7 +93,8 @@ static void choose_segments(const mcl_engine *e, FusedPlan &P, int sms) {
     const long long items = tiles * nseg;
     const double waves = (double)items / slots;
     const double eff = waves / std::ceil(waves);
-    const double score = eff * seg_len / (seg_len + 4.0 * 0.35);  // extra planes mostly hit L2
+    const double extra = C.kind ? 2.0 * 0.15 : 4.0 * 0.35;  // extra planes mostly hit L2
+    const double score = eff * seg_len / (seg_len + extra);
     if (score > best_score + 1e-9) {
       best_score = score;
       best = nseg;
@@ -99,12 +105,12 @@ static void choose_segments(const mcl_engine *e, FusedPlan &P, int sms) {
 }
 
 static int choose_cfg(const mcl_engine *e) {
-  // smaller lattices (few tiles) favour the 2-CTA configuration; large planes the 30-row tiles
-  long long area = 0;
-  for (auto &D : e->desc) area += (long long)D.nx * D.ny;
+  // Colour passes (faster than the fused kernel on every measured workload): 3 CTAs per SM fit the 80 registers
+  // of the non-flip kernels; flip models (a second trial per site) need the 2-CTA variant's registers.
   const char *env = getenv("MCL_FUSED_CFG");
   if (env) return std::max(0, std::min(kNumCfgs - 1, atoi(env)));
-  return area >= 128ll * 128 ? 1 : 0;
+  const bool flip = e->model.flip != 0 || e->model.potential == POT_PEAR;
+  return flip ? 4 : 2;
 }
 
 static int prepare_kernel(mcl_engine *e, FusedPlan *P);
@@ -116,7 +122,7 @@ static int build_items(mcl_engine *e, FusedPlan *P) {
   std::vector<CUtensorMap> maps(2 * e->n_rep);
   for (int r = 0; r < e->n_rep; r++)
     for (int b = 0; b < 2; b++) {
-      int rc = encode_map(&maps[2 * r + b], e->d_dir[b], e->desc[r], P->ty);
+      int rc = encode_map(&maps[2 * r + b], e->d_dir[b], e->desc[r], P->ty + (kCfgs[P->cfg].kind ? 2 : 4));
       if (rc) return rc;
     }
   cudaFree(P->d_tmaps);
@@ -141,8 +147,10 @@ static int build_items(mcl_engine *e, FusedPlan *P) {
   CKF(cudaMalloc(&P->d_first, first.size() * sizeof(int)));
   CKF(cudaMemcpy(P->d_first, first.data(), first.size() * sizeof(int), cudaMemcpyHostToDevice));
   CKF(cudaMalloc(&P->d_partials, (size_t)P->n_items * kPartials * sizeof(double)));
-  const size_t slot_floats = ((size_t)3 * RW * (P->ty + 4) + 31) / 32 * 32;
-  P->smem = 128 + (size_t)NSL * slot_floats * sizeof(float) + NSL * sizeof(unsigned long long);
+  const bool pass = kCfgs[P->cfg].kind == 1;
+  const int nsl = pass ? NSLP : NSL;
+  const size_t slot_floats = ((size_t)3 * RW * (P->ty + (pass ? 2 : 4)) + 31) / 32 * 32;
+  P->smem = 128 + (size_t)nsl * slot_floats * sizeof(float) + nsl * sizeof(unsigned long long);
   return prepare_kernel(e, P);
 }
 
@@ -233,6 +241,11 @@ static FusedLaunch launch_desc(const mcl_engine *e, const FusedPlan *P) {
 }
 
 static cudaError_t dispatch(const mcl_engine *e, const FusedArgs &a, const FusedLaunch &l) {
+  if (kCfgs[l.cfg].kind == 1) {
+    if (e->model.potential == POT_GHRL) return launch_pass_ghrl(e->model, a, l);
+    if (e->model.potential == POT_PEAR) return launch_pass_pear(e->model, a, l);
+    return launch_pass_ll(e->model, a, l);
+  }
   if (e->model.potential == POT_GHRL) return launch_fused_ghrl(e->model, a, l);
   if (e->model.potential == POT_PEAR) return launch_fused_pear(e->model, a, l);
   return launch_fused_ll(e->model, a, l);
@@ -249,11 +262,14 @@ static int prepare_kernel(mcl_engine *e, FusedPlan *P) {
   return MCL_OK;
 }
 
+int fused_launches_per_sweep(const mcl_engine *e) { return e->fused && kCfgs[e->fused->cfg].kind == 1 ? 3 : 2; }
+
 int fused_sweep(mcl_engine *e, bool measure, cudaEvent_t ev0, cudaEvent_t ev1) {
   FusedPlan *P = e->fused;
+  const bool pass = kCfgs[P->cfg].kind == 1;
   FusedArgs a;
   a.tmaps = P->d_tmaps;
-  a.out = e->d_dir[e->cur ^ 1];
+  a.out = e->d_dir[pass ? e->cur : e->cur ^ 1];  // colour passes update in place
   a.reps = e->d_desc;
   a.st = e->d_state;
   a.items = P->d_items;
@@ -264,13 +280,24 @@ int fused_sweep(mcl_engine *e, bool measure, cudaEvent_t ev0, cudaEvent_t ev1) {
   a.measure = measure ? 1 : 0;
   a.timeout_ns = P->timeout_ns;
   a.skip_first_load = P->skip_first_load;
+  a.colour = 0;
   if (ev0) CKF(cudaEventRecord(ev0, e->stream));
   const FusedLaunch l = launch_desc(e, P);
-  const cudaError_t err = dispatch(e, a, l);
-  if (err != cudaSuccess) return cuda_fail(err, "fused sweep launch");
+  if (pass) {  // colour 0 without measurement, then colour 1 with the observables of the whole lattice
+    FusedArgs a0 = a;
+    a0.measure = 0;
+    cudaError_t err = dispatch(e, a0, l);
+    if (err != cudaSuccess) return cuda_fail(err, "colour pass launch");
+    a.colour = 1;
+    err = dispatch(e, a, l);
+    if (err != cudaSuccess) return cuda_fail(err, "colour pass launch");
+  } else {
+    const cudaError_t err = dispatch(e, a, l);
+    if (err != cudaSuccess) return cuda_fail(err, "fused sweep launch");
+    e->cur ^= 1;
+  }
   if (ev1) CKF(cudaEventRecord(ev1, e->stream));
-  e->cur ^= 1;
-  e->launches += 2;
+  e->launches += fused_launches_per_sweep(e);
   BlockTable t;
   t.first = P->d_first;
   LaunchCtx c = e->ctx();

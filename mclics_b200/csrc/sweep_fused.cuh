@@ -49,6 +49,7 @@ struct FusedArgs {
   int measure;                  // fuse the observables
   long long timeout_ns;
   int skip_first_load;          // test hook: never issue the first TMA load (its wait must time out)
+  int colour;                   // colour-pass kernel: the colour updated (0: x + y + z even)
 };
 
 constexpr int TXF = 64, HALF = 40, RW = 2 * HALF, NPAIR = 16, NSL = 7;
@@ -196,9 +197,15 @@ __device__ __forceinline__ void pair_task(const ModelDev &m, const Ctx &c, float
   const SiteResultT<float2> r =
       site_update<POT, FLIP, PXY, CHIRAL, FIELD, float2>(m, n, nb, w, sid, sn, c.elecE, ld, c.av, c.T, c.invT);
   const float2 nx2[3] = {r.n.x, r.n.y, r.n.z};
+  // Only the updated lanes go back: along a periodic x with nx % 4 == 2 the right ring site shares its pair of cells
+  // with the tile's last row pair, whose second lane is outside the lattice — two tasks, one lane each.
+  if (v0 && v1) {
 #pragma unroll
-  for (int q = 0; q < 3; q++)
-    *reinterpret_cast<float2 *>(own + q * PF) = make_float2(v0 ? nx2[q].x : o[q].x, v1 ? nx2[q].y : o[q].y);
+    for (int q = 0; q < 3; q++) *reinterpret_cast<float2 *>(own + q * PF) = nx2[q];
+  } else {
+#pragma unroll
+    for (int q = 0; q < 3; q++) own[q * PF + (v0 ? 0 : 1)] = v0 ? nx2[q].x : nx2[q].y;
+  }
   if (count) accepted += (v0 && r.rot.x ? 1u : 0u) + (v1 && r.rot.y ? 1u : 0u);
   if (meas) {
     const float2 eb = __ffma2_rn(make_float2(2.f, 2.f), r.bond, r.single);
@@ -532,11 +539,12 @@ __global__ void __launch_bounds__(NT, NT <= 256 ? 2 : 1) k_sweep_fused(ModelDev 
   }
 }
 
-// Tile configurations: rows per tile and threads per CTA (64 columns always).
+// Tile configurations: rows per tile, threads per CTA (64 columns always), resident CTAs per SM, and the kernel:
+// kind 0 the fused two-colour sweep (this file), kind 1 two colour passes (sweep_pass.cuh).
 struct FusedCfg {
-  int ty, nt, ctas_per_sm;
+  int ty, nt, ctas_per_sm, kind;
 };
-constexpr int kNumCfgs = 2;
+constexpr int kNumCfgs = 5;
 
 // Launch of one potential's kernels (sweep_fused_{ll,ghrl,pear}.cu): dispatch over geometry, flip, periodic x/y,
 // chirality, field and tile configuration.
@@ -551,6 +559,9 @@ struct FusedLaunch {
 cudaError_t launch_fused_ll(const ModelDev &m, const FusedArgs &a, const FusedLaunch &l);
 cudaError_t launch_fused_ghrl(const ModelDev &m, const FusedArgs &a, const FusedLaunch &l);
 cudaError_t launch_fused_pear(const ModelDev &m, const FusedArgs &a, const FusedLaunch &l);
+cudaError_t launch_pass_ll(const ModelDev &m, const FusedArgs &a, const FusedLaunch &l);
+cudaError_t launch_pass_ghrl(const ModelDev &m, const FusedArgs &a, const FusedLaunch &l);
+cudaError_t launch_pass_pear(const ModelDev &m, const FusedArgs &a, const FusedLaunch &l);
 
 template <int POT, int GEO, bool FLIP, bool PXY, bool CHIRAL, bool FIELD, int TY, int NT>
 cudaError_t launch_fused_one(const ModelDev &m, const FusedArgs &a, const FusedLaunch &l) {

@@ -38,6 +38,7 @@ def test_autotune_restores_the_state_and_keeps_the_physics():
     before = snapshot(e)
     t = e.autotune(2)
     assert t["candidates"] >= 2 and t["threads_per_cta"] in (256, 512) and t["work_items"] > 0
+    assert 0 <= t["tile_config"] <= 4
     assert t["ms_per_sweep"] <= t["ms_default"] * (1 + 1e-9)
     after = snapshot(e)
     for a, b in zip(before[0], after[0]):
@@ -49,12 +50,15 @@ def test_autotune_restores_the_state_and_keeps_the_physics():
     twin.sweeps(5, measure=True)
     for r in range(len(SIZES)):
         assert np.array_equal(e.download(r), twin.download(r)), r  # same site arithmetic whatever the tiling
-        np.testing.assert_allclose(e.series(r)["energy"], twin.series(r)["energy"], rtol=1e-12, atol=0)
+        # the plan may change the kernel (fused or colour passes) and with it the FP32 grouping of the site terms
+        np.testing.assert_allclose(e.series(r)["energy"], twin.series(r)["energy"], rtol=2e-6, atol=0)
     e.close()
     twin.close()
 
 
-def test_graph_replay_matches_direct_launches():
+@pytest.mark.parametrize("cfg", ["1", "2"], ids=["fused", "pass"])
+def test_graph_replay_matches_direct_launches(cfg, monkeypatch):
+    monkeypatch.setenv("MCL_FUSED_CFG", cfg)
     a, b = make(), make()
     b.set_graphs(True)
     for n, meas in [(7, True), (4, False), (3, True)]:
@@ -71,5 +75,26 @@ def test_graph_replay_matches_direct_launches():
         assert np.array_equal(a.download(r), b.download(r)), r
         sa, sb = a.series(r), b.series(r)
         assert sa.tobytes() == sb.tobytes(), r
+    a.close()
+    b.close()
+
+
+def test_set_plan_applies_a_plan_and_keeps_the_physics():
+    a, b = make(), make()
+    b.set_plan(3, 8)
+    p = b.plan()
+    assert (p["tile_config"], p["rows_per_tile"], p["threads_per_cta"], p["planes_per_segment"]) == (3, 32, 512, 8)
+    assert p["work_items"] > 0
+    with pytest.raises(M.McLicsError) as ei:
+        b.set_plan(5, 0)
+    assert ei.value.code == 1
+    b.set_graphs(True)
+    for e in (a, b):
+        e.sweeps(4, measure=True)
+    b.set_plan(0, 0)  # back to the fused kernel mid-run: the ping-pong buffers take over from the in-place state
+    for e in (a, b):
+        e.sweeps(3, measure=True)
+    for r in range(len(SIZES)):
+        assert np.array_equal(a.download(r), b.download(r)), r
     a.close()
     b.close()

@@ -1,10 +1,26 @@
-"""The fused tiled sweep (TMA plane streaming, both colours per pass, ghost cells, ping-pong buffers) against
-the untiled two-colour kernel: same Philox draws, same physics code, so the two must agree site by site on every
-geometry the tiling has to get right (ragged last tiles, several z segments, free and periodic axes, tiny
-lattices, batches of replicas of different sizes). Also the bounded TMA wait: a withheld copy makes the wait run
-out, the error is reported at the next synchronising call and the engine keeps working."""
+"""The tiled sweeps on TMA-streamed planes — the fused kernel (both colours per pass over HBM, ghost cells,
+ping-pong buffers) and the in-place colour passes — against the untiled two-colour kernel: same Philox draws, same
+physics code, so they must agree site by site on every geometry the tiling has to get right (ragged last tiles,
+several z segments, free and periodic axes, tiny lattices, batches of replicas of different sizes). The colour
+passes must reproduce the fused kernel bit for bit in every tile configuration. Also the bounded TMA wait: a
+withheld copy makes the wait run out, the error is reported at the next synchronising call and the engine keeps
+working."""
 import numpy as np
 import pytest
+
+# tile configurations (MCL_FUSED_CFG): "0", "1" = fused kernel (64 x 14, 64 x 28 tiles), "2"-"4" = colour passes
+KERNELS = {"fused14": "0", "fused28": "1", "pass": "2"}
+PASS_CFGS = ["2", "3", "4"]
+
+
+@pytest.fixture
+def kernel_cfg(monkeypatch, request):
+    cfg = request.param
+    if cfg is None:
+        monkeypatch.delenv("MCL_FUSED_CFG", raising=False)
+    else:
+        monkeypatch.setenv("MCL_FUSED_CFG", cfg)
+    return cfg
 
 from helpers import M
 
@@ -31,7 +47,8 @@ SHAPES = [
     (72, 22, 70, "bulk", (1, 1, 1)),       # ragged x and y tiles, several z segments
     (30, 18, 26, "bulk", (0, 0, 0)),       # free everywhere, odd-free sizes
     (2, 2, 2, "bulk", (1, 1, 1)),          # smallest periodic lattice: ghosts of ghosts
-    (6, 4, 4, "bulk", (1, 0, 1)),
+    (6, 4, 4, "bulk", (1, 0, 1)),          # periodic nx % 4 == 2: the right ring site shares a pair of cells
+    (66, 12, 10, "bulk", (1, 1, 1)),       # ... also in a second x tile
     (68, 20, 33, "slab", (1, 1, 0)),
     (16, 16, 1, "slab", (1, 1, 0)),        # single plane (surface 1 only)
     (130, 34, 12, "slab", (0, 1, 0)),
@@ -51,12 +68,10 @@ def run(model, reps, schedule, sweeps, measure, seeds):
     return out, ser, av
 
 
-@pytest.mark.gpu
-@pytest.mark.parametrize("model", sorted(MODELS))
-@pytest.mark.parametrize("shape", SHAPES, ids=["%dx%dx%d-%s-%s" % (s[0], s[1], s[2], s[3], "".join(map(str, s[4])))
-                                               for s in SHAPES])
-def test_fused_equals_untiled(model, shape):
-    nx, ny, nz, geo, per = shape
+SHAPE_IDS = ["%dx%dx%d-%s-%s" % (s[0], s[1], s[2], s[3], "".join(map(str, s[4]))) for s in SHAPES]
+
+
+def model_for(model, geo):
     if geo == "bulk" and model in ("ghrl_slab", "ghrl_chiral_rp", "pear_field"):
         m = MODELS[model]()
         m.n_surfaces = 0
@@ -64,6 +79,16 @@ def test_fused_equals_untiled(model, shape):
         m = MODELS[model]()
     if geo == "slab" and m.n_surfaces < 2:
         m = M.Model("ll", surfaces=[("homeotropic", 1.0, 0, 0), ("fg", 0.5, 0, 0)])
+    return m
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel_cfg", list(KERNELS.values()), ids=list(KERNELS), indirect=True)
+@pytest.mark.parametrize("model", sorted(MODELS))
+@pytest.mark.parametrize("shape", SHAPES, ids=SHAPE_IDS)
+def test_fused_equals_untiled(model, shape, kernel_cfg):
+    nx, ny, nz, geo, per = shape
+    m = model_for(model, geo)
     reps = [M.Replica(nx, ny, nz, geo, per, T=0.9, seed=99)]
     a, sa, ava = run(m, reps, M.SCHED_CHECKER2, 4, True, [5])
     b, sb, avb = run(m, reps, M.SCHED_CHECKER2_SIMPLE, 4, True, [5])
@@ -76,7 +101,28 @@ def test_fused_equals_untiled(model, shape):
 
 
 @pytest.mark.gpu
-def test_fused_batch_of_uneven_replicas():
+@pytest.mark.parametrize("cfg", PASS_CFGS)
+@pytest.mark.parametrize("model", sorted(MODELS))
+@pytest.mark.parametrize("shape", SHAPES, ids=SHAPE_IDS)
+def test_colour_passes_equal_fused_bitwise(model, shape, cfg, monkeypatch):
+    nx, ny, nz, geo, per = shape
+    m = model_for(model, geo)
+    reps = [M.Replica(nx, ny, nz, geo, per, T=0.9, seed=99)]
+    monkeypatch.setenv("MCL_FUSED_CFG", "1")
+    a, sa, ava = run(m, reps, M.SCHED_CHECKER2, 5, True, [5])
+    monkeypatch.setenv("MCL_FUSED_CFG", cfg)
+    b, sb, avb = run(m, reps, M.SCHED_CHECKER2, 5, True, [5])
+    np.testing.assert_array_equal(a[0], b[0])
+    assert ava == avb
+    np.testing.assert_allclose(sa[0]["energy"], sb[0]["energy"], rtol=2e-6, atol=2e-6)
+    np.testing.assert_allclose(sa[0]["q"], sb[0]["q"], rtol=0, atol=2e-7)
+    np.testing.assert_allclose(sa[0]["nsum"], sb[0]["nsum"], rtol=1e-6, atol=1e-4)
+    np.testing.assert_array_equal(sa[0]["acceptance"], sb[0]["acceptance"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel_cfg", list(KERNELS.values()), ids=list(KERNELS), indirect=True)
+def test_fused_batch_of_uneven_replicas(kernel_cfg):
     m = M.Model("ll")
     sizes = [(16, 16, 16), (24, 24, 24), (40, 18, 30), (8, 8, 8), (64, 32, 20)]
     reps = [M.Replica(*s, T=1.0 + 0.05 * i, seed=100 + i) for i, s in enumerate(sizes)]
@@ -89,7 +135,8 @@ def test_fused_batch_of_uneven_replicas():
 
 
 @pytest.mark.gpu
-def test_ghosts_and_buffers_survive_alternating_paths():
+@pytest.mark.parametrize("kernel_cfg", list(KERNELS.values()), ids=list(KERNELS), indirect=True)
+def test_ghosts_and_buffers_survive_alternating_paths(kernel_cfg):
     """Fused sweeps, then untiled ones (decision recording forces them), then fused again: the ghost cells and the
     ping-pong buffers stay consistent with an engine that used the untiled path throughout."""
     m = M.Model("ghrl", k=(1.0, 0.5, 1.5))
@@ -109,7 +156,8 @@ def test_ghosts_and_buffers_survive_alternating_paths():
 
 
 @pytest.mark.gpu
-def test_tma_wait_timeout_reports_and_recovers():
+@pytest.mark.parametrize("kernel_cfg", list(KERNELS.values()), ids=list(KERNELS), indirect=True)
+def test_tma_wait_timeout_reports_and_recovers(kernel_cfg):
     m = M.Model("ll")
     rp = M.Replica(64, 32, 32, "bulk", (1, 1, 1), T=1.0, seed=1)
     e = M.Engine(m, [rp], M.SCHED_CHECKER2)
