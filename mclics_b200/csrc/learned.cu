@@ -313,7 +313,7 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_forward_tc(const MlpTC *__restr
                                                             float *__restrict__ out, unsigned *__restrict__ err,
                                                             long long timeout_ns) {
   extern __shared__ __align__(128) unsigned char tc_dyn[];
-  TcSmem &S = *reinterpret_cast<TcSmem *>(((uintptr_t)tc_dyn + 127) & ~(uintptr_t)127);
+  TcSmem &S = *reinterpret_cast<TcSmem *>(tc_align128(tc_dyn));
   tc_setup(S, w);
   unsigned phase = 0;
   for (long long base = (long long)blockIdx.x * kTcRows; base < n; base += (long long)gridDim.x * kTcRows) {
@@ -438,7 +438,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_sweep_learned(ModelDev m, const
                                                             int measure, double *__restrict__ partials) {
   extern __shared__ __align__(128) unsigned char ls_dyn[];
   __shared__ double red[kThreads / 32][kPartials];
-  unsigned char *sbase = (unsigned char *)(((uintptr_t)ls_dyn + 127) & ~(uintptr_t)127);
+  unsigned char *sbase = tc_align128(ls_dyn);
   MlpDev *S = nullptr;
   __nv_bfloat16(*As)[32][24] = nullptr;
   float(*Out)[32][4] = nullptr;

@@ -51,6 +51,12 @@ struct TcSmem {
 
 __device__ __forceinline__ uint32_t tc_smem(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
+// A dynamic shared-memory array rounded up to 128 bytes by an offset from the array itself, so that accesses
+// through the result stay in the shared address space.
+__device__ __forceinline__ unsigned char *tc_align128(unsigned char *base) {
+  return base + ((128u - (tc_smem(base) & 127u)) & 127u);
+}
+
 __device__ __forceinline__ uint64_t tc_desc(const void *start, uint32_t lbo, uint32_t sbo) {
   return (uint64_t)((tc_smem(start) & 0x3FFFFu) >> 4) | ((uint64_t)(lbo >> 4) << 16) |
          ((uint64_t)(sbo >> 4) << 32) | (1ull << 46);

@@ -62,6 +62,12 @@ struct Win {
 // ---- PTX helpers -----------------------------------------------------------------------------------------
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 
+// The dynamic shared-memory window rounded up to 128 bytes, as an offset from the shared array itself: the
+// compiler keeps the shared address space (LDS/STS; an integer round trip would make every access generic).
+__device__ __forceinline__ unsigned char *smem_align128(unsigned char *base) {
+  return base + ((128u - (smem_u32(base) & 127u)) & 127u);
+}
+
 __device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
@@ -100,12 +106,24 @@ __device__ __forceinline__ void tma_load_plane(float *dst, const CUtensorMap *ma
       : "memory");
 }
 
+// try_wait with a suspend-time hint: a thread whose phase is not complete sleeps (up to hint_ns) instead of
+// returning at once, so waiting warps take no issue slots.
+__device__ __forceinline__ bool mbar_try_wait_sleep(unsigned long long *bar, unsigned parity, unsigned hint_ns) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
+      : "memory");
+  return ok != 0;
+}
+
 // Bounded wait for the barrier's phase `parity`; false on timeout.
 __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, unsigned parity, long long timeout_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const unsigned long long t0 = globaltimer();
   while (true) {
-    if (mbar_try_wait(bar, parity)) return true;
+    if (mbar_try_wait_sleep(bar, parity, 100000u)) return true;
     if ((long long)(globaltimer() - t0) > timeout_ns) return false;
   }
 }
@@ -287,7 +305,7 @@ __global__ void __launch_bounds__(NT, NT <= 256 ? 2 : 1) k_sweep_fused(ModelDev 
   constexpr int PF = Win<TY>::PF, SLOT = Win<TY>::SLOT;
   static_assert((TY + 2) * NPAIR + TY + TY * NPAIR <= 2 * NT, "two task slots per thread must cover a step");
   extern __shared__ __align__(128) unsigned char smem_dyn[];
-  unsigned char *smem_raw = (unsigned char *)(((uintptr_t)smem_dyn + 127) & ~(uintptr_t)127);
+  unsigned char *smem_raw = smem_align128(smem_dyn);
   float *slots = reinterpret_cast<float *>(smem_raw);
   unsigned long long *bars = reinterpret_cast<unsigned long long *>(smem_raw + (size_t)NSL * SLOT * 4);
   __shared__ int s_fail;
@@ -327,14 +345,14 @@ __global__ void __launch_bounds__(NT, NT <= 256 ? 2 : 1) k_sweep_fused(ModelDev 
   const int pbeg = z0 - 2, pend = z1 + 1;
   auto plane_exists = [&](int p) { return perz || (p >= 0 && p < nz); };
   auto wrapz = [&](int p) { return p < 0 ? p + nz : (p >= nz ? p - nz : p); };
-  auto slot_ptr = [&](int p) -> float * { return slots + (size_t)((p - pbeg) % NSL) * SLOT; };
+  auto slot_ptr = [&](int p) -> float * { return slots + (size_t)((unsigned)(p - pbeg) % NSL) * SLOT; };
   int last_issued = pbeg - 1;  // meaningful in thread 0 only
   auto issue = [&](int p) {    // thread 0 only
     if (p > pend) return;
     const int lp = p - pbeg;
     last_issued = p;
     if (a.skip_first_load && lp == 0) return;  // test hook: nothing will complete this barrier phase
-    unsigned long long *bar = &bars[lp % NSL];
+    unsigned long long *bar = &bars[(unsigned)lp % NSL];
     if (!plane_exists(p)) {  // no copy: complete the slot's phase anyway
       mbar_arrive(bar);
       return;
@@ -346,7 +364,8 @@ __global__ void __launch_bounds__(NT, NT <= 256 ? 2 : 1) k_sweep_fused(ModelDev 
   auto wait_plane = [&](int p) -> bool {
     if (p <= pend && p > waited) {
       const int lp = p - pbeg;
-      if (plane_exists(p) && !mbar_wait_bounded(&bars[lp % NSL], (unsigned)((lp / NSL) & 1), a.timeout_ns)) s_fail = 1;
+      if (plane_exists(p) && !mbar_wait_bounded(&bars[(unsigned)lp % NSL], ((unsigned)lp / NSL) & 1u, a.timeout_ns))
+        s_fail = 1;
     }
     __syncthreads();
     if (s_fail) return false;
@@ -511,7 +530,7 @@ __global__ void __launch_bounds__(NT, NT <= 256 ? 2 : 1) k_sweep_fused(ModelDev 
       for (int p = max(waited + 1, last_issued - NSL + 1); p <= last_issued; p++) {
         if (!plane_exists(p) || (a.skip_first_load && p == pbeg)) continue;
         const int lp = p - pbeg;
-        mbar_wait_bounded(&bars[lp % NSL], (unsigned)((lp / NSL) & 1), a.timeout_ns);
+        mbar_wait_bounded(&bars[(unsigned)lp % NSL], ((unsigned)lp / NSL) & 1u, a.timeout_ns);
       }
     }
     __syncthreads();

@@ -11,13 +11,15 @@
 // shared-memory slots; each slot is one 5-D TMA box (40 half-row cells, 2 parities, TY + 2 rows, 1 plane, 3
 // components) of the split layout, completed on an mbarrier. At step k (plane k) thread (row r, pair p) updates the
 // two colour-c sites x and x + 2 of row y0 + r (adjacent cells of one half-row, paired FP32 lanes, one Philox call),
-// reading plane k for the in-plane neighbours and planes k - 1, k + 1 for the z neighbours, and stores the pair to
-// global memory with the ghost copies of edge sites. Plane k + 2 is loaded meanwhile into the slot of plane k - 2.
+// reading plane k for the in-plane neighbours and plane k + 1 for the +z neighbours, and stores the pair to global
+// memory with the ghost copies of edge sites. The -z neighbours (plane k - 1, the same cells in the parity of the
+// step-k sites) are the other-parity cells the thread read at step k - 1, kept in registers, so plane k - 1 leaves
+// shared memory before step k: planes k + 2 and k + 3 are in flight while step k runs.
 //
 // Measurement (colour-1 pass): every bond has exactly one colour-1 end, so E_total = sum_1 (2 bond + single) +
-// sum_0 single; the colour-1 task also adds Q and sum n of its two updated sites and of the two colour-0 sites of
-// the same cells in the other half-row (final since the colour-0 pass). Site terms are summed in FP32 per task and
-// step, then in FP64.
+// sum_0 single; the colour-1 task also adds the raw moments (sum n_a n_b, sum n) of its two updated sites and of
+// the two colour-0 sites of the same cells in the other half-row (final since the colour-0 pass), summed in FP32
+// per task and step, then in FP64; each thread turns its moments into sum Q = 1.5 sum n_a n_b - 0.5 delta_ab N.
 //
 // Every wait on a TMA barrier is bounded by %globaltimer; on timeout the CTA sets the error word, waits (bounded)
 // for its copies in flight and returns, and the host reports MCL_ERR_CUDA.
@@ -57,26 +59,18 @@ static __device__ __noinline__ void pass_ghosts(float *row0, long long cs, int p
   }
 }
 
-// Site terms of the observables for a pair of sites (lanes with valid = false contribute nothing).
-__device__ __forceinline__ void add_site_terms(float (&f)[kPartials], const float2 (&v)[3], bool ok0, bool ok1) {
-  const float2 z2 = make_float2(0.f, 0.f);
-  const float2 vx = make_float2(ok0 ? v[0].x : 0.f, ok1 ? v[0].y : 0.f);
-  const float2 vy = make_float2(ok0 ? v[1].x : 0.f, ok1 ? v[1].y : 0.f);
-  const float2 vz = make_float2(ok0 ? v[2].x : 0.f, ok1 ? v[2].y : 0.f);
-  const float2 h = make_float2(1.5f, 1.5f);
-  const float2 c = make_float2(ok0 ? -0.5f : 0.f, ok1 ? -0.5f : 0.f);
-  const float2 hx = __fmul2_rn(h, vx), hy = __fmul2_rn(h, vy);
-  const float2 q1 = __ffma2_rn(hx, vx, c), q2 = __ffma2_rn(hx, vy, z2), q3 = __ffma2_rn(hx, vz, z2);
-  const float2 q4 = __ffma2_rn(hy, vy, c), q5 = __ffma2_rn(hy, vz, z2), q6 = __ffma2_rn(__fmul2_rn(h, vz), vz, c);
-  f[1] += q1.x + q1.y;
-  f[2] += q2.x + q2.y;
-  f[3] += q3.x + q3.y;
-  f[4] += q4.x + q4.y;
-  f[5] += q5.x + q5.y;
-  f[6] += q6.x + q6.y;
-  f[7] += vx.x + vx.y;
-  f[8] += vy.x + vy.y;
-  f[9] += vz.x + vz.y;
+// Raw moments of two pairs of sites (lanes paired): m[0..5] = sum v_a v_b (xx, xy, xz, yy, yz, zz), m[6..8] = sum v.
+// Q and sum n follow per thread at the end: sum q_ab = 1.5 sum v_a v_b - 0.5 delta_ab (sites).
+__device__ __forceinline__ void pair_moments(float2 (&m)[9], const float2 (&u)[3], const float2 (&v)[3]) {
+  m[0] = __ffma2_rn(v[0], v[0], __fmul2_rn(u[0], u[0]));
+  m[1] = __ffma2_rn(v[0], v[1], __fmul2_rn(u[0], u[1]));
+  m[2] = __ffma2_rn(v[0], v[2], __fmul2_rn(u[0], u[2]));
+  m[3] = __ffma2_rn(v[1], v[1], __fmul2_rn(u[1], u[1]));
+  m[4] = __ffma2_rn(v[1], v[2], __fmul2_rn(u[1], u[2]));
+  m[5] = __ffma2_rn(v[2], v[2], __fmul2_rn(u[2], u[2]));
+  m[6] = __fadd2_rn(u[0], v[0]);
+  m[7] = __fadd2_rn(u[1], v[1]);
+  m[8] = __fadd2_rn(u[2], v[2]);
 }
 
 template <int POT, int GEO, bool FLIP, bool PXY, bool CHIRAL, bool FIELD, int TY, int NT, int MINB>
@@ -84,7 +78,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_pass(ModelDev m, FusedArgs a
   constexpr int PF = PassWin<TY>::PF, SLOT = PassWin<TY>::SLOT;
   static_assert(NT == TY * NPAIR, "one pair task per thread and plane");
   extern __shared__ __align__(128) unsigned char smem_dyn[];
-  unsigned char *smem_raw = (unsigned char *)(((uintptr_t)smem_dyn + 127) & ~(uintptr_t)127);
+  unsigned char *smem_raw = smem_align128(smem_dyn);
   float *slots = reinterpret_cast<float *>(smem_raw);
   unsigned long long *bars = reinterpret_cast<unsigned long long *>(smem_raw + (size_t)NSLP * SLOT * 4);
   __shared__ int s_fail;
@@ -125,14 +119,14 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_pass(ModelDev m, FusedArgs a
   const int pbeg = z0 - 1, pend = z1;
   auto plane_exists = [&](int p) { return perz || (p >= 0 && p < nz); };
   auto wrapz = [&](int p) { return p < 0 ? p + nz : (p >= nz ? p - nz : p); };
-  auto slot_ptr = [&](int p) -> float * { return slots + (size_t)((p - pbeg) % NSLP) * SLOT; };
+  auto slot_ptr = [&](int p) -> float * { return slots + (size_t)((unsigned)(p - pbeg) % NSLP) * SLOT; };
   int last_issued = pbeg - 1;  // meaningful in thread 0 only
   auto issue = [&](int p) {    // thread 0 only
     if (p > pend) return;
     const int lp = p - pbeg;
     last_issued = p;
     if (a.skip_first_load && lp == 0) return;  // test hook: nothing will complete this barrier phase
-    unsigned long long *bar = &bars[lp % NSLP];
+    unsigned long long *bar = &bars[(unsigned)lp % NSLP];
     if (!plane_exists(p)) {  // no copy: complete the slot's phase anyway
       mbar_arrive(bar);
       return;
@@ -144,7 +138,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_pass(ModelDev m, FusedArgs a
   auto wait_plane = [&](int p) -> bool {
     if (p <= pend && p > waited) {
       const int lp = p - pbeg;
-      if (plane_exists(p) && !mbar_wait_bounded(&bars[lp % NSLP], (unsigned)((lp / NSLP) & 1), a.timeout_ns))
+      if (plane_exists(p) && !mbar_wait_bounded(&bars[(unsigned)lp % NSLP], ((unsigned)lp / NSLP) & 1u, a.timeout_ns))
         s_fail = 1;
     }
     __syncthreads();
@@ -152,12 +146,14 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_pass(ModelDev m, FusedArgs a
     if (p > waited) waited = p;
     return true;
   };
-  // Slot reuse: step k reads planes k-1 .. k+1; plane k+2 goes into the slot of plane k-2, whose last reader was
-  // step k-1 (the barrier at the start of step k separates them).
+  // Slot reuse: step k reads planes k and k + 1 only (the -z neighbours of a task are the other-parity cells the
+  // same thread read at step k - 1, carried in registers); plane k + 3 goes into the slot of plane k - 1, whose last
+  // reader was step k - 1 (the barrier at the start of step k separates them). Two planes are in flight meanwhile.
   if (tid == 0)
-    for (int p = pbeg; p <= pbeg + 2; p++) issue(p);
+    for (int p = pbeg; p <= pbeg + 3; p++) issue(p);
 
   unsigned accepted = 0;
+  int n_meas = 0;  // sites whose raw moments this thread summed
   double dacc[kPartials];
 #pragma unroll
   for (int q = 0; q < kPartials; q++) dacc[q] = 0.0;
@@ -171,24 +167,36 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_pass(ModelDev m, FusedArgs a
   const bool live_row = y < ny;
 
   bool ok = wait_plane(z0 - 1) && wait_plane(z0);
+  // -z neighbours of the first step: plane z0 - 1, row y, the parity of this thread's sites in plane z0
+  float2 pd[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+  if (ok && live_row && plane_exists(z0 - 1)) {
+    const float *q0 = slot_ptr(z0 - 1) + ((r + 1) * 2 + ((colour + y + z0) & 1)) * HALF + jb;
+#pragma unroll
+    for (int q = 0; q < 3; q++) pd[q] = *reinterpret_cast<const float2 *>(q0 + q * PF);
+  }
   for (int k = z0; ok && k < z1; k++) {
     ok = wait_plane(k + 1);
     if (!ok) break;
-    if (tid == 0) issue(k + 2);
-    if (!live_row || !plane_exists(k)) continue;
+    if (tid == 0) issue(k + 3);
+    if (!live_row) continue;
     const int h = (colour + y + k) & 1;
     const int x = x0 + 4 * p + h;
     const bool v0 = x < nx, v1 = x + 2 < nx;
-    if (!v0) continue;
     const float *cs_k = slot_ptr(k);
-    const float *below = plane_exists(k - 1) ? slot_ptr(k - 1) : nullptr;
+    // the other-parity cells of the pair are the -z neighbours of the next step's pair (same cells, plane k)
+    const float *pn_src = cs_k + ((r + 1) * 2 + (h ^ 1)) * HALF + jb;
+    if (!v0) {
+#pragma unroll
+      for (int q = 0; q < 3; q++) pd[q] = *reinterpret_cast<const float2 *>(pn_src + q * PF);
+      continue;
+    }
+    const bool has_below = plane_exists(k - 1);
     const float *above = plane_exists(k + 1) ? slot_ptr(k + 1) : nullptr;
     const int zw = wrapz(k);
     const float *own = cs_k + ((r + 1) * 2 + h) * HALF + jb;
     const float *oth = cs_k + ((r + 1) * 2 + (h ^ 1)) * HALF + jb - 1 + h;  // 3 consecutive cells
     const float *zu = above ? above + ((r + 1) * 2 + h) * HALF + jb : own;
-    const float *zd = below ? below + ((r + 1) * 2 + h) * HALF + jb : own;
-    float2 o[3], yu[3], yd[3], pu[3], pd[3];
+    float2 o[3], yu[3], yd[3], pu[3];
     float xa[3], xb[3], xc[3];
 #pragma unroll
     for (int q = 0; q < 3; q++) {
@@ -196,7 +204,6 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_pass(ModelDev m, FusedArgs a
       yu[q] = *reinterpret_cast<const float2 *>(own + q * PF + RW);
       yd[q] = *reinterpret_cast<const float2 *>(own + q * PF - RW);
       pu[q] = *reinterpret_cast<const float2 *>(zu + q * PF);
-      pd[q] = *reinterpret_cast<const float2 *>(zd + q * PF);
       xa[q] = oth[q * PF];
       xb[q] = oth[q * PF + 1];
       xc[q] = oth[q * PF + 2];
@@ -233,7 +240,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_pass(ModelDev m, FusedArgs a
       w[2] = make_float2(wyp, wyp);
       w[3] = make_float2(wym, wym);
     }
-    const float wzu = above ? 1.f : 0.f, wzd = below ? 1.f : 0.f;
+    const float wzu = above ? 1.f : 0.f, wzd = has_below ? 1.f : 0.f;
     w[4] = make_float2(wzu, wzu);
     w[5] = make_float2(wzd, wzd);
     const SiteResultT<float2> res =
@@ -256,29 +263,43 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_pass(ModelDev m, FusedArgs a
       pass_ghosts(row0, cs, R.px, fin[0].x, fin[1].x, fin[2].x, fin[0].y, fin[1].y, fin[2].y, v1, jl, nx, ny, y,
                   c.perx, c.pery);
     accepted += (res.rot.x ? 1u : 0u) + (v1 && res.rot.y ? 1u : 0u);
+    float2 pn[3];
+#pragma unroll
+    for (int q = 0; q < 3; q++) pn[q] = *reinterpret_cast<const float2 *>(pn_src + q * PF);
     if (measure) {
-      float f[kPartials];
       const float2 eb = __ffma2_rn(make_float2(2.f, 2.f), res.bond, res.single);
-      f[0] = v1 ? eb.x + eb.y : eb.x;
+      float e = v1 ? eb.x + eb.y : eb.x;
+      // the colour-0 sites in the same cells of the other half-row (pn): x0 + 4 p + (h ^ 1) + 2 e
+      float2 va[3], vb[3];
 #pragma unroll
-      for (int q = 1; q < kPartials; q++) f[q] = 0.f;
-      add_site_terms(f, fin, true, v1);
-      // the colour-0 sites in the same cells of the other half-row: x0 + 4 p + (h ^ 1) + 2 e
-      const float *pa = cs_k + ((r + 1) * 2 + (h ^ 1)) * HALF + jb;
-      float2 va[3];
-#pragma unroll
-      for (int q = 0; q < 3; q++) va[q] = *reinterpret_cast<const float2 *>(pa + q * PF);
+      for (int q = 0; q < 3; q++) {
+        va[q] = pn[q];
+        vb[q] = fin[q];
+      }
       const int xa0 = x0 + 4 * p + (h ^ 1);
       const bool a0 = xa0 < nx, a1 = xa0 + 2 < nx;
-      add_site_terms(f, va, a0, a1);
       if (sid >= 0 || (FIELD && m.field_on)) {
         const float2 sa = single_energy<FIELD>(m, V3<float2>{va[0], va[1], va[2]}, sid, sn, c.elecE);
-        if (a0) f[0] += sa.x;
-        if (a1) f[0] += sa.y;
+        if (a0) e += sa.x;
+        if (a1) e += sa.y;
       }
+      if (!(v1 && a0 && a1)) {  // ragged right edge: lanes outside the lattice count nothing
 #pragma unroll
-      for (int q = 0; q < kPartials; q++) dacc[q] += (double)f[q];
+        for (int q = 0; q < 3; q++) {
+          vb[q].y = v1 ? vb[q].y : 0.f;
+          va[q].x = a0 ? va[q].x : 0.f;
+          va[q].y = a1 ? va[q].y : 0.f;
+        }
+      }
+      n_meas += 1 + (int)v1 + (int)a0 + (int)a1;
+      float2 mo[9];
+      pair_moments(mo, vb, va);
+      dacc[0] += (double)e;
+#pragma unroll
+      for (int q = 0; q < 9; q++) dacc[q + 1] += (double)(mo[q].x + mo[q].y);
     }
+#pragma unroll
+    for (int q = 0; q < 3; q++) pd[q] = pn[q];
   }
 
   if (!ok) {
@@ -287,7 +308,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_pass(ModelDev m, FusedArgs a
       for (int q = max(waited + 1, last_issued - NSLP + 1); q <= last_issued; q++) {
         if (!plane_exists(q) || (a.skip_first_load && q == pbeg)) continue;
         const int lp = q - pbeg;
-        mbar_wait_bounded(&bars[lp % NSLP], (unsigned)((lp / NSLP) & 1), a.timeout_ns);
+        mbar_wait_bounded(&bars[(unsigned)lp % NSLP], ((unsigned)lp / NSLP) & 1u, a.timeout_ns);
       }
     }
     __syncthreads();
@@ -297,6 +318,12 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_pass(ModelDev m, FusedArgs a
   const unsigned wsum = __reduce_add_sync(0xffffffffu, accepted);
   if ((tid & 31) == 0 && wsum) atomicAdd(&a.st[it.rep].acc, (unsigned long long)wsum);
   if (measure) {
+    // raw moments -> sum of q = 1.5 v_a v_b - 0.5 delta_ab (partials 1..6: xx, xy, xz, yy, yz, zz)
+#pragma unroll
+    for (int q = 1; q <= 6; q++) dacc[q] *= 1.5;
+    dacc[1] -= 0.5 * n_meas;
+    dacc[4] -= 0.5 * n_meas;
+    dacc[6] -= 0.5 * n_meas;
     __shared__ double red[NT / 32][kPartials];
     const int lane = tid & 31, warp = tid >> 5;
 #pragma unroll
