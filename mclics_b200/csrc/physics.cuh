@@ -179,11 +179,20 @@ __device__ __forceinline__ L field_energy(const ModelDev &m, const V3<L> &x, flo
   return fma_(splat<L>(-m.elecA), mul_(ne, ne), mul_(splat<L>(-m.elecP), ne));
 }
 
-// Anchoring of surface sid for a site with outward normal s (src/anchoring_*.cpp surface_potential, W included).
-__device__ __forceinline__ float anchoring_energy(const ModelDev &m, int sid, const Vec3 &x, const Vec3 &s) {
-  const float W = m.anch_W[sid];
-  const Vec3 lab{m.anch_lab[sid][0], m.anch_lab[sid][1], m.anch_lab[sid][2]};
-  switch (m.anch_type[sid]) {
+// Anchoring of one surface for a site with outward normal s (src/anchoring_*.cpp surface_potential, W included).
+// Not inlined: surface sites are rare, and the seven anchoring forms would otherwise claim registers in every
+// sweep kernel's hot loop. Arguments by value (a reference to the kernel's model parameter would force a copy).
+static __device__ __noinline__ float anchoring_core(int type, float W, float lx, float ly, float lz, float lam, float mu,
+                                                    float nu, float rho, float sigma, float x0, float x1, float x2,
+                                                    float s0, float s1, float s2) {
+  ModelDev m;  // only the GHRL coefficients are read below
+  m.lam = lam;
+  m.mu = mu;
+  m.nu = nu;
+  m.rho = rho;
+  m.sigma = sigma;
+  const Vec3 x{x0, x1, x2}, s{s0, s1, s2}, lab{lx, ly, lz};
+  switch (type) {
     case ANCH_HOMEOTROPIC: {
       const float c = dot(x, s);
       return __fmul_rn(-W, __fmul_rn(c, c));
@@ -219,6 +228,11 @@ __device__ __forceinline__ float anchoring_energy(const ModelDev &m, int sid, co
     }
   }
   return 0.f;
+}
+
+__device__ __forceinline__ float anchoring_energy(const ModelDev &m, int sid, const Vec3 &x, const Vec3 &s) {
+  return anchoring_core(m.anch_type[sid], m.anch_W[sid], m.anch_lab[sid][0], m.anch_lab[sid][1], m.anch_lab[sid][2],
+                        m.lam, m.mu, m.nu, m.rho, m.sigma, x.x, x.y, x.z, s.x, s.y, s.z);
 }
 
 // Single-site terms: anchoring (sid >= 0, the same surface for both lanes) and, with FIELD, the field (FIELD is
@@ -315,8 +329,10 @@ __device__ __forceinline__ V3<L> sel3(LB<L> c, const V3<L> &a, const V3<L> &b) {
 
 // One trial move (src/evolve.cpp:133-207): rotation, Metropolis, then the optional n -> -n trial.
 // Compile-time features: FLIP (n -> -n trial), PXY (x, y neighbours always present), CHIRAL (GHRL sigma term),
-// FIELD (field term). Every combination rounds like the general one on the inputs it applies to.
-template <int POT, bool FLIP, bool PXY, bool CHIRAL, bool FIELD, typename L>
+// FIELD (field term), SINGLE = false (the caller knows the site has no single-site term: no surface, no field;
+// the energies are then the bond sums themselves, which is what adding the zero single term gives, up to the sign
+// of a zero). Every combination rounds like the general one on the inputs it applies to.
+template <int POT, bool FLIP, bool PXY, bool CHIRAL, bool FIELD, typename L, bool SINGLE = true>
 __device__ __forceinline__ SiteResultT<L> site_update(const ModelDev &m, const V3<L> &n, const V3<L> (&nb)[6],
                                                       const L (&w)[6], int sid, const Vec3 &s, float elecE,
                                                       const LaneDraw<L> &d, float av, float T, float invT) {
@@ -324,18 +340,20 @@ __device__ __forceinline__ SiteResultT<L> site_update(const ModelDev &m, const V
   const V3<L> nn = rotate_trial(n, va, d.w0, d.w1, d.w2);
   L b_old, b_new;
   bond_sum2<POT, PXY, CHIRAL>(m, n, nn, nb, w, b_old, b_new);
-  const L s_old = single_energy<FIELD>(m, n, sid, s, elecE), s_new = single_energy<FIELD>(m, nn, sid, s, elecE);
-  const L e_old = add_(b_old, s_old), e_new = add_(b_new, s_new);
+  const L s_old = SINGLE ? single_energy<FIELD>(m, n, sid, s, elecE) : splat<L>(0.f);
+  const L s_new = SINGLE ? single_energy<FIELD>(m, nn, sid, s, elecE) : splat<L>(0.f);
+  const L e_old = SINGLE ? add_(b_old, s_old) : b_old, e_new = SINGLE ? add_(b_new, s_new) : b_new;
   SiteResultT<L> r;
   r.rot = metropolis(d.u3, sub_(e_new, e_old), invT, T);
   r.n = sel3<L>(r.rot, nn, n);
   r.bond = sel_(r.rot, b_new, b_old);
-  r.single = sel_(r.rot, s_new, s_old);
+  r.single = SINGLE ? sel_(r.rot, s_new, s_old) : splat<L>(0.f);
   if (FLIP) {
     const V3<L> f{neg_(r.n.x), neg_(r.n.y), neg_(r.n.z)};
-    const L bf = bond_sum<POT, PXY, CHIRAL>(m, f, nb, w), sf = single_energy<FIELD>(m, f, sid, s, elecE);
-    const L e_cur = add_(r.bond, r.single);
-    r.flip = metropolis(d.u4, sub_(add_(bf, sf), e_cur), invT, T);
+    const L bf = bond_sum<POT, PXY, CHIRAL>(m, f, nb, w);
+    const L sf = SINGLE ? single_energy<FIELD>(m, f, sid, s, elecE) : splat<L>(0.f);
+    const L e_cur = SINGLE ? add_(r.bond, r.single) : r.bond;
+    r.flip = metropolis(d.u4, SINGLE ? sub_(add_(bf, sf), e_cur) : sub_(bf, e_cur), invT, T);
     r.n = sel3<L>(r.flip, f, r.n);
     r.bond = sel_(r.flip, bf, r.bond);
     r.single = sel_(r.flip, sf, r.single);

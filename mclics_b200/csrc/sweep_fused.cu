@@ -12,9 +12,10 @@
 
 namespace mcl {
 
-// 0, 1: fused (7 slots of TY + 4 rows: one CTA per SM either way); 2-4: colour passes (4 slots of TY + 2 rows).
+// 0, 1: fused (7 slots of TY + 4 rows: one CTA per SM either way); 2-5: colour passes (4 slots of TY + 2 rows;
+// 5 runs two pair tasks per thread).
 static const FusedCfg kCfgs[kNumCfgs] = {{14, 256, 1, 0}, {28, 512, 1, 0}, {16, 256, 3, 1}, {32, 512, 1, 1},
-                                         {16, 256, 2, 1}};
+                                         {16, 256, 2, 1}, {16, 128, 3, 1}};
 
 struct FusedPlan {
   int cfg = 0, tx = 64, ty = 14, seg = 32;

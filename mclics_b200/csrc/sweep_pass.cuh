@@ -24,6 +24,8 @@
 // Every wait on a TMA barrier is bounded by %globaltimer; on timeout the CTA sets the error word, waits (bounded)
 // for its copies in flight and returns, and the host reports MCL_ERR_CUDA.
 #pragma once
+#include <type_traits>
+
 #include "sweep_fused.cuh"
 
 namespace mcl {
@@ -73,10 +75,11 @@ __device__ __forceinline__ void pair_moments(float2 (&m)[9], const float2 (&u)[3
   m[8] = __fadd2_rn(u[2], v[2]);
 }
 
-template <int POT, int GEO, bool FLIP, bool PXY, bool CHIRAL, bool FIELD, int TY, int NT, int MINB>
+template <int POT, int GEO, bool FLIP, bool PXY, bool CHIRAL, bool FIELD, int TY, int NT, int MINB, int TPT>
 __global__ void __launch_bounds__(NT, MINB) k_sweep_pass(ModelDev m, FusedArgs a) {
   constexpr int PF = PassWin<TY>::PF, SLOT = PassWin<TY>::SLOT;
-  static_assert(NT == TY * NPAIR, "one pair task per thread and plane");
+  static_assert(NT * TPT == TY * NPAIR, "TPT pair tasks per thread and plane");
+  static_assert(TPT == 1 || (TY / TPT) % 2 == 0, "a thread's rows must share their parity pattern");
   extern __shared__ __align__(128) unsigned char smem_dyn[];
   unsigned char *smem_raw = smem_align128(smem_dyn);
   float *slots = reinterpret_cast<float *>(smem_raw);
@@ -158,148 +161,187 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_pass(ModelDev m, FusedArgs a
 #pragma unroll
   for (int q = 0; q < kPartials; q++) dacc[q] = 0.0;
 
-  const int r = tid >> 4, p = tid & 15;  // task: row y0 + r, pair p
-  const int y = y0 + r;
-  const int jb = 4 + 2 * p;  // window cell of the pair's first site
+  // tasks of this thread: pair p of rows rr[t] = r0 + t TY / TPT (same parity pattern: TY / TPT is even)
+  const int r0 = tid >> 4, p = tid & 15;
+  int rr[TPT];
+  bool live[TPT];
+#pragma unroll
+  for (int t = 0; t < TPT; t++) {
+    rr[t] = r0 + t * (TY / TPT);
+    live[t] = y0 + rr[t] < ny;
+  }
+  const int jb = 4 + 2 * p;   // window cell of the pair's first site
   const int jl = j0 + 2 * p;  // half index of the pair's first site
-  const int yw = y;  // rows of a tile never wrap (y < ny for live tasks)
   const long long cs = R.comp;
-  const bool live_row = y < ny;
 
   bool ok = wait_plane(z0 - 1) && wait_plane(z0);
   // -z neighbours of the first step: plane z0 - 1, row y, the parity of this thread's sites in plane z0
-  float2 pd[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
-  if (ok && live_row && plane_exists(z0 - 1)) {
-    const float *q0 = slot_ptr(z0 - 1) + ((r + 1) * 2 + ((colour + y + z0) & 1)) * HALF + jb;
+  float2 pd[TPT][3];
 #pragma unroll
-    for (int q = 0; q < 3; q++) pd[q] = *reinterpret_cast<const float2 *>(q0 + q * PF);
+  for (int t = 0; t < TPT; t++) {
+#pragma unroll
+    for (int q = 0; q < 3; q++) pd[t][q] = make_float2(0.f, 0.f);
+    if (ok && live[t] && plane_exists(z0 - 1)) {
+      const float *q0 = slot_ptr(z0 - 1) + ((rr[t] + 1) * 2 + ((colour + y0 + rr[t] + z0) & 1)) * HALF + jb;
+#pragma unroll
+      for (int q = 0; q < 3; q++) pd[t][q] = *reinterpret_cast<const float2 *>(q0 + q * PF);
+    }
   }
   for (int k = z0; ok && k < z1; k++) {
     ok = wait_plane(k + 1);
     if (!ok) break;
     if (tid == 0) issue(k + 3);
-    if (!live_row) continue;
-    const int h = (colour + y + k) & 1;
+    if (!live[0]) continue;  // rows grow with t: a dead first row has no live rows after it
+    const int h = (colour + y0 + r0 + k) & 1;
     const int x = x0 + 4 * p + h;
     const bool v0 = x < nx, v1 = x + 2 < nx;
     const float *cs_k = slot_ptr(k);
-    // the other-parity cells of the pair are the -z neighbours of the next step's pair (same cells, plane k)
-    const float *pn_src = cs_k + ((r + 1) * 2 + (h ^ 1)) * HALF + jb;
-    if (!v0) {
+    if (!v0) {  // the other-parity cells are still the next step's -z neighbours
 #pragma unroll
-      for (int q = 0; q < 3; q++) pd[q] = *reinterpret_cast<const float2 *>(pn_src + q * PF);
+      for (int t = 0; t < TPT; t++)
+        if (live[t]) {
+          const float *src = cs_k + ((rr[t] + 1) * 2 + (h ^ 1)) * HALF + jb;
+#pragma unroll
+          for (int q = 0; q < 3; q++) pd[t][q] = *reinterpret_cast<const float2 *>(src + q * PF);
+        }
       continue;
     }
-    const bool has_below = plane_exists(k - 1);
-    const float *above = plane_exists(k + 1) ? slot_ptr(k + 1) : nullptr;
-    const int zw = wrapz(k);
-    const float *own = cs_k + ((r + 1) * 2 + h) * HALF + jb;
-    const float *oth = cs_k + ((r + 1) * 2 + (h ^ 1)) * HALF + jb - 1 + h;  // 3 consecutive cells
-    const float *zu = above ? above + ((r + 1) * 2 + h) * HALF + jb : own;
-    float2 o[3], yu[3], yd[3], pu[3];
-    float xa[3], xb[3], xc[3];
+    // Surface planes and field models take the general path; everything else has no single-site term (bulk
+    // without a field: never). With one task per thread a slab runs the general path on every plane (a second copy
+    // of the update costs registers that the 3-CTA configuration does not have; the runtime surface test then
+    // makes the site terms zero).
+    constexpr bool kNever = GEO == GEO_BULK && !FIELD, kAlways = FIELD || (GEO == GEO_SLAB && TPT == 1);
+    const bool single_terms = kNever ? false : (kAlways ? true : (k == 0 || k == nz - 1));
+    auto step = [&](auto single_tag) {
+      constexpr bool SINGLE = decltype(single_tag)::value;
+      const bool has_below = plane_exists(k - 1);
+      const float *above = plane_exists(k + 1) ? slot_ptr(k + 1) : nullptr;
+      const int zw = k;  // computed planes lie inside the lattice
+      int sid = -1;
+      float sz = 0.f;
+      if (SINGLE && GEO == GEO_SLAB) sid = slab_surface(zw, nz, sz);
+      const Vec3 sn{0.f, 0.f, sz};
+      float2 o[TPT][3];
+      SiteResultT<float2> res[TPT];
 #pragma unroll
-    for (int q = 0; q < 3; q++) {
-      o[q] = *reinterpret_cast<const float2 *>(own + q * PF);
-      yu[q] = *reinterpret_cast<const float2 *>(own + q * PF + RW);
-      yd[q] = *reinterpret_cast<const float2 *>(own + q * PF - RW);
-      pu[q] = *reinterpret_cast<const float2 *>(zu + q * PF);
-      xa[q] = oth[q * PF];
-      xb[q] = oth[q * PF + 1];
-      xc[q] = oth[q * PF + 2];
-    }
-    int sid = -1;
-    float sz = 0.f;
-    if (GEO == GEO_SLAB) sid = slab_surface(zw, nz, sz);
-    const Vec3 sn{0.f, 0.f, sz};
-    Draw d0, d1;
-    if (FLIP) {
-      d0 = site_draw(c.seed, c.sweep, x, yw, zw, nx, ny, true);
-      d1 = site_draw(c.seed, c.sweep, x + 2, yw, zw, nx, ny, true);
-    } else {  // one Philox call serves both sites (x & ~2 is shared: x % 4 = h)
-      const U4 out = site_draws(c.seed, c.sweep, pair_counter(x, yw, zw, nx, ny), 0);
-      d0 = pair_half(out, 0u);
-      d1 = pair_half(out, 1u);
-    }
-    const LaneDraw<float2> ld = lane_draw(d0, d1, FLIP);
-    const V3<float2> n{o[0], o[1], o[2]};
-    const V3<float2> nb[6] = {
-        V3<float2>{make_float2(xb[0], xc[0]), make_float2(xb[1], xc[1]), make_float2(xb[2], xc[2])},  // +x
-        V3<float2>{make_float2(xa[0], xb[0]), make_float2(xa[1], xb[1]), make_float2(xa[2], xb[2])},  // -x
-        V3<float2>{yu[0], yu[1], yu[2]},
-        V3<float2>{yd[0], yd[1], yd[2]},
-        V3<float2>{pu[0], pu[1], pu[2]},
-        V3<float2>{pd[0], pd[1], pd[2]}};
-    float2 w[6];
-    if (PXY) {
-      w[0] = w[1] = w[2] = w[3] = make_float2(1.f, 1.f);
-    } else {
-      const float wyp = (c.pery || y + 1 < ny) ? 1.f : 0.f, wym = (c.pery || y - 1 >= 0) ? 1.f : 0.f;
-      w[0] = make_float2((c.perx || x + 1 < nx) ? 1.f : 0.f, (c.perx || x + 3 < nx) ? 1.f : 0.f);
-      w[1] = make_float2((c.perx || x - 1 >= 0) ? 1.f : 0.f, 1.f);
-      w[2] = make_float2(wyp, wyp);
-      w[3] = make_float2(wym, wym);
-    }
-    const float wzu = above ? 1.f : 0.f, wzd = has_below ? 1.f : 0.f;
-    w[4] = make_float2(wzu, wzu);
-    w[5] = make_float2(wzd, wzd);
-    const SiteResultT<float2> res =
-        site_update<POT, FLIP, PXY, CHIRAL, FIELD, float2>(m, n, nb, w, sid, sn, c.elecE, ld, c.av, c.T, c.invT);
-    const float2 fin[3] = {make_float2(res.n.x.x, v1 ? res.n.x.y : o[0].y),
-                           make_float2(res.n.y.x, v1 ? res.n.y.y : o[1].y),
-                           make_float2(res.n.z.x, v1 ? res.n.z.y : o[2].y)};
-    // in-place store of the pair (half-row of parity h of row y, plane zw), then the ghosts of edge sites
-    float *row0 = a.out + R.off + ((long long)zw * R.py + (y + GY)) * R.px + h * R.hp + GH;
-    if (v1) {
-#pragma unroll
-      for (int q = 0; q < 3; q++) *reinterpret_cast<float2 *>(row0 + q * cs + jl) = fin[q];
-    } else {
-#pragma unroll
-      for (int q = 0; q < 3; q++) row0[q * cs + jl] = fin[q].x;
-    }
-    const bool gx = c.perx && (jl == 0 || jl + 1 >= (nx >> 1) - 1);
-    const bool gy = c.pery && (y < 2 || y >= ny - 2);
-    if (gx || gy)
-      pass_ghosts(row0, cs, R.px, fin[0].x, fin[1].x, fin[2].x, fin[0].y, fin[1].y, fin[2].y, v1, jl, nx, ny, y,
-                  c.perx, c.pery);
-    accepted += (res.rot.x ? 1u : 0u) + (v1 && res.rot.y ? 1u : 0u);
-    float2 pn[3];
-#pragma unroll
-    for (int q = 0; q < 3; q++) pn[q] = *reinterpret_cast<const float2 *>(pn_src + q * PF);
-    if (measure) {
-      const float2 eb = __ffma2_rn(make_float2(2.f, 2.f), res.bond, res.single);
-      float e = v1 ? eb.x + eb.y : eb.x;
-      // the colour-0 sites in the same cells of the other half-row (pn): x0 + 4 p + (h ^ 1) + 2 e
-      float2 va[3], vb[3];
-#pragma unroll
-      for (int q = 0; q < 3; q++) {
-        va[q] = pn[q];
-        vb[q] = fin[q];
-      }
-      const int xa0 = x0 + 4 * p + (h ^ 1);
-      const bool a0 = xa0 < nx, a1 = xa0 + 2 < nx;
-      if (sid >= 0 || (FIELD && m.field_on)) {
-        const float2 sa = single_energy<FIELD>(m, V3<float2>{va[0], va[1], va[2]}, sid, sn, c.elecE);
-        if (a0) e += sa.x;
-        if (a1) e += sa.y;
-      }
-      if (!(v1 && a0 && a1)) {  // ragged right edge: lanes outside the lattice count nothing
+      for (int t = 0; t < TPT; t++) {
+        const int y = y0 + rr[t];
+        const float *own = cs_k + ((rr[t] + 1) * 2 + h) * HALF + jb;
+        const float *oth = cs_k + ((rr[t] + 1) * 2 + (h ^ 1)) * HALF + jb - 1 + h;  // 3 consecutive cells
+        const float *zu = above ? above + ((rr[t] + 1) * 2 + h) * HALF + jb : own;
+        float2 yu[3], yd[3], pu[3];
+        float xa[3], xb[3], xc[3];
 #pragma unroll
         for (int q = 0; q < 3; q++) {
-          vb[q].y = v1 ? vb[q].y : 0.f;
-          va[q].x = a0 ? va[q].x : 0.f;
-          va[q].y = a1 ? va[q].y : 0.f;
+          o[t][q] = *reinterpret_cast<const float2 *>(own + q * PF);
+          yu[q] = *reinterpret_cast<const float2 *>(own + q * PF + RW);
+          yd[q] = *reinterpret_cast<const float2 *>(own + q * PF - RW);
+          pu[q] = *reinterpret_cast<const float2 *>(zu + q * PF);
+          xa[q] = oth[q * PF];
+          xb[q] = oth[q * PF + 1];
+          xc[q] = oth[q * PF + 2];
         }
+        Draw d0, d1;
+        if (FLIP) {
+          d0 = site_draw(c.seed, c.sweep, x, y, zw, nx, ny, true);
+          d1 = site_draw(c.seed, c.sweep, x + 2, y, zw, nx, ny, true);
+        } else {  // one Philox call serves both sites (x & ~2 is shared: x % 4 = h)
+          const U4 out = site_draws(c.seed, c.sweep, pair_counter(x, y, zw, nx, ny), 0);
+          d0 = pair_half(out, 0u);
+          d1 = pair_half(out, 1u);
+        }
+        const LaneDraw<float2> ld = lane_draw(d0, d1, FLIP);
+        const V3<float2> n{o[t][0], o[t][1], o[t][2]};
+        const V3<float2> nb[6] = {
+            V3<float2>{make_float2(xb[0], xc[0]), make_float2(xb[1], xc[1]), make_float2(xb[2], xc[2])},  // +x
+            V3<float2>{make_float2(xa[0], xb[0]), make_float2(xa[1], xb[1]), make_float2(xa[2], xb[2])},  // -x
+            V3<float2>{yu[0], yu[1], yu[2]},
+            V3<float2>{yd[0], yd[1], yd[2]},
+            V3<float2>{pu[0], pu[1], pu[2]},
+            V3<float2>{pd[t][0], pd[t][1], pd[t][2]}};
+        float2 w[6];
+        if (PXY) {
+          w[0] = w[1] = w[2] = w[3] = make_float2(1.f, 1.f);
+        } else {
+          const float wyp = (c.pery || y + 1 < ny) ? 1.f : 0.f, wym = (c.pery || y - 1 >= 0) ? 1.f : 0.f;
+          w[0] = make_float2((c.perx || x + 1 < nx) ? 1.f : 0.f, (c.perx || x + 3 < nx) ? 1.f : 0.f);
+          w[1] = make_float2((c.perx || x - 1 >= 0) ? 1.f : 0.f, 1.f);
+          w[2] = make_float2(wyp, wyp);
+          w[3] = make_float2(wym, wym);
+        }
+        const float wzu = above ? 1.f : 0.f, wzd = has_below ? 1.f : 0.f;
+        w[4] = make_float2(wzu, wzu);
+        w[5] = make_float2(wzd, wzd);
+        res[t] = site_update<POT, FLIP, PXY, CHIRAL, FIELD, float2, SINGLE>(m, n, nb, w, sid, sn, c.elecE, ld, c.av,
+                                                                           c.T, c.invT);
       }
-      n_meas += 1 + (int)v1 + (int)a0 + (int)a1;
-      float2 mo[9];
-      pair_moments(mo, vb, va);
-      dacc[0] += (double)e;
 #pragma unroll
-      for (int q = 0; q < 9; q++) dacc[q + 1] += (double)(mo[q].x + mo[q].y);
-    }
+      for (int t = 0; t < TPT; t++) {
+        if (!live[t]) continue;
+        const int y = y0 + rr[t];
+        const float2 fin[3] = {make_float2(res[t].n.x.x, v1 ? res[t].n.x.y : o[t][0].y),
+                               make_float2(res[t].n.y.x, v1 ? res[t].n.y.y : o[t][1].y),
+                               make_float2(res[t].n.z.x, v1 ? res[t].n.z.y : o[t][2].y)};
+        // in-place store of the pair (half-row of parity h of row y, plane zw), then the ghosts of edge sites
+        float *row0 = a.out + R.off + ((long long)zw * R.py + (y + GY)) * R.px + h * R.hp + GH;
+        if (v1) {
 #pragma unroll
-    for (int q = 0; q < 3; q++) pd[q] = pn[q];
+          for (int q = 0; q < 3; q++) *reinterpret_cast<float2 *>(row0 + q * cs + jl) = fin[q];
+        } else {
+#pragma unroll
+          for (int q = 0; q < 3; q++) row0[q * cs + jl] = fin[q].x;
+        }
+        const bool gx = c.perx && (jl == 0 || jl + 1 >= (nx >> 1) - 1);
+        const bool gy = c.pery && (y < 2 || y >= ny - 2);
+        if (gx || gy)
+          pass_ghosts(row0, cs, R.px, fin[0].x, fin[1].x, fin[2].x, fin[0].y, fin[1].y, fin[2].y, v1, jl, nx, ny, y,
+                      c.perx, c.pery);
+        accepted += (res[t].rot.x ? 1u : 0u) + (v1 && res[t].rot.y ? 1u : 0u);
+        // the other-parity cells of the pair: the colour-0 sites measured below, and the next step's -z neighbours
+        const float *pn_src = cs_k + ((rr[t] + 1) * 2 + (h ^ 1)) * HALF + jb;
+        float2 pn[3];
+#pragma unroll
+        for (int q = 0; q < 3; q++) pn[q] = *reinterpret_cast<const float2 *>(pn_src + q * PF);
+        if (measure) {
+          const float2 eb = __ffma2_rn(make_float2(2.f, 2.f), res[t].bond, res[t].single);
+          float e = v1 ? eb.x + eb.y : eb.x;
+          // the colour-0 sites in the same cells of the other half-row (pn): x0 + 4 p + (h ^ 1) + 2 e
+          float2 va[3], vb[3];
+#pragma unroll
+          for (int q = 0; q < 3; q++) {
+            va[q] = pn[q];
+            vb[q] = fin[q];
+          }
+          const int xa0 = x0 + 4 * p + (h ^ 1);
+          const bool a0 = xa0 < nx, a1 = xa0 + 2 < nx;
+          if (SINGLE) {
+            const float2 sa = single_energy<FIELD>(m, V3<float2>{va[0], va[1], va[2]}, sid, sn, c.elecE);
+            if (a0) e += sa.x;
+            if (a1) e += sa.y;
+          }
+          if (!(v1 && a0 && a1)) {  // ragged right edge: lanes outside the lattice count nothing
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+              vb[q].y = v1 ? vb[q].y : 0.f;
+              va[q].x = a0 ? va[q].x : 0.f;
+              va[q].y = a1 ? va[q].y : 0.f;
+            }
+          }
+          n_meas += 1 + (int)v1 + (int)a0 + (int)a1;
+          float2 mo[9];
+          pair_moments(mo, vb, va);
+          dacc[0] += (double)e;
+#pragma unroll
+          for (int q = 0; q < 9; q++) dacc[q + 1] += (double)(mo[q].x + mo[q].y);
+        }
+#pragma unroll
+        for (int q = 0; q < 3; q++) pd[t][q] = pn[q];
+      }
+    };
+    if (single_terms)
+      step(std::true_type{});
+    else
+      step(std::false_type{});
   }
 
   if (!ok) {
@@ -342,21 +384,23 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_pass(ModelDev m, FusedArgs a
   }
 }
 
-template <int POT, int GEO, bool FLIP, bool PXY, bool CHIRAL, bool FIELD, int TY, int NT, int MINB>
+template <int POT, int GEO, bool FLIP, bool PXY, bool CHIRAL, bool FIELD, int TY, int NT, int MINB, int TPT>
 cudaError_t launch_pass_one(const ModelDev &m, const FusedArgs &a, const FusedLaunch &l) {
-  auto k = k_sweep_pass<POT, GEO, FLIP, PXY, CHIRAL, FIELD, TY, NT, MINB>;
+  auto k = k_sweep_pass<POT, GEO, FLIP, PXY, CHIRAL, FIELD, TY, NT, MINB, TPT>;
   if (l.prepare) return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)l.smem);
   k<<<l.n_items, NT, l.smem, l.stream>>>(m, a);
   return cudaGetLastError();
 }
 
 // Pass tile configurations (cfg numbering continues the fused kernel's): 2: 64 x 16, 256 threads, 3 CTAs/SM;
-// 3: 64 x 32, 512 threads, 1 CTA/SM; 4: 64 x 16, 256 threads, 2 CTAs/SM.
+// 3: 64 x 32, 512 threads, 1 CTA/SM; 4: 64 x 16, 256 threads, 2 CTAs/SM; 5: 64 x 16, 128 threads with two pair
+// tasks each (rows r and r + 8), 3 CTAs/SM.
 template <int POT, int GEO, bool FLIP, bool PXY, bool CHIRAL, bool FIELD>
 cudaError_t launch_pass_cfg(const ModelDev &m, const FusedArgs &a, const FusedLaunch &l) {
-  if (l.cfg == 3) return launch_pass_one<POT, GEO, FLIP, PXY, CHIRAL, FIELD, 32, 512, 1>(m, a, l);
-  if (l.cfg == 4) return launch_pass_one<POT, GEO, FLIP, PXY, CHIRAL, FIELD, 16, 256, 2>(m, a, l);
-  return launch_pass_one<POT, GEO, FLIP, PXY, CHIRAL, FIELD, 16, 256, 3>(m, a, l);
+  if (l.cfg == 3) return launch_pass_one<POT, GEO, FLIP, PXY, CHIRAL, FIELD, 32, 512, 1, 1>(m, a, l);
+  if (l.cfg == 4) return launch_pass_one<POT, GEO, FLIP, PXY, CHIRAL, FIELD, 16, 256, 2, 1>(m, a, l);
+  if (l.cfg == 5) return launch_pass_one<POT, GEO, FLIP, PXY, CHIRAL, FIELD, 16, 128, 3, 2>(m, a, l);
+  return launch_pass_one<POT, GEO, FLIP, PXY, CHIRAL, FIELD, 16, 256, 3, 1>(m, a, l);
 }
 
 template <int POT, bool FLIP, bool CHIRAL, bool FIELD>
