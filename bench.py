@@ -118,14 +118,17 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(kernel_key):
-    """Per-launch DRAM traffic of a kernel from the committed ncu summary (profiles/ncu_traffic.json), or None."""
+def ncu_traffic(workload, tile_config):
+    """Per-launch DRAM bytes of the sweep kernel from the committed ncu summary (profiles/ncu_traffic.json), when
+    the summary was taken with the same kernel kind (colour passes: tile configurations 2-5) as this run."""
     p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if not os.path.exists(p):
         return None
     with open(p) as f:
-        d = json.load(f)
-    return d.get(kernel_key)
+        d = json.load(f).get(workload)
+    if not d or (int(d["plan"].split(",")[0]) >= 2) != (tile_config >= 2):
+        return None
+    return d["dram_bytes_per_launch"]
 
 
 class ClockSampler:
@@ -518,6 +521,9 @@ def main():
     value = sites_total * args.steps / (res["dev_ms"] / 1e3)
     e2e = sites_total * args.steps / (res["e2e_ms"] / 1e3)
     peak, peak_kind = measured_peaks()
+    # per launch: a sweep is 2 colour-pass launches (each half the site updates) or 1 fused launch; the ratio of
+    # algorithmic bytes to time is the same either way
+    launches_per_sweep = 2 if tu["tile_config"] >= 2 else 1
     achieved = res["sites"] * BYTES_PER_SITE_UPDATE / (res["kernel_ms"] / 1e3) / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": "site-updates/s", "n_gpus": world, "steps": args.steps,
@@ -528,7 +534,11 @@ def main():
                 "d2h_bytes_per_step": 144 * res["n_rep"] + 12 * res["sites"]},
         "gpu_launches": res["launches"],
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": peak_kind, "traffic": ncu_traffic(args.workload),
+                     "peak_kind": peak_kind, "traffic": ncu_traffic(args.workload, tu["tile_config"]),
+                     "traffic_kind": "ncu dram read + write bytes per launch, cold L2 (profiles/ncu_traffic.json)",
+                     "launches_per_sweep": launches_per_sweep,
+                     "kernel_ms_per_launch": res["kernel_ms"] / launches_per_sweep,
+                     "algorithmic_bytes_per_launch": res["sites"] * BYTES_PER_SITE_UPDATE / launches_per_sweep,
                      "kernel_ms_per_sweep": res["kernel_ms"],
                      "algorithmic_bytes_per_sweep": res["sites"] * BYTES_PER_SITE_UPDATE},
         "cpu_baseline": cpu,
