@@ -206,6 +206,29 @@ int mcl_autotune(mcl_engine *e, int trial_sweeps, mcl_tuning *out);
  * choose. mcl_get_plan fills the plan fields of *out (tile_config .. work_items; the timing fields are 0). */
 int mcl_set_plan(mcl_engine *e, int tile_config, int planes_per_segment);
 int mcl_get_plan(mcl_engine *e, mcl_tuning *out);
+
+/* ---- Z-slab decomposition: one lattice over several processes, one GPU each (no counterpart in the reference,
+ * which sweeps one lattice in one process on one GPU, src/evolve.cu:317-440) --------------------------------------
+ * A process owns the global planes z_offset .. z_offset + nz_own - 1 of a lattice of nz_global planes. Its engine
+ * has one replica (bulk or slab geometry) created with nz = nz_own + 2 and a free z axis; local planes 0 and
+ * nz - 1 are halo copies of the neighbouring processes' boundary planes, and periodic_z gives the global z
+ * boundary. Site draws and slab surfaces use global plane indices, so the processes together take exactly the
+ * decisions one engine sweeping the whole lattice takes. The engine runs the colour-pass kernel; the caller moves
+ * the boundary planes between processes (e.g. NCCL send/recv over NVLink) and sums the observables. One sweep:
+ *   for colour 0, 1: mcl_zslab_pass(colour); mcl_zslab_pack(send_lo, send_hi); exchange; mcl_zslab_unpack(...)
+ *   mcl_zslab_sums(measure, sums); sum the sums over the processes; mcl_zslab_finalize(sums, measure)
+ * where send_lo (the lowest owned plane) goes to the lower neighbour's recv_hi and send_hi to the upper neighbour's
+ * recv_lo. Before the first sweep, pack, exchange and unpack once. Buffers are device memory the caller owns:
+ * plane buffers of *plane_floats floats ([component][padded row][cell], ghost cells included), sums of 11 doubles
+ * (energy, Q xx xy xz yy yz zz, sum n, accepted rotations). Every call is asynchronous on the engine's stream.
+ * A z-slab engine refuses mcl_sweeps, mcl_measure and mcl_autotune; the directors it downloads are its nz_own + 2
+ * local planes. */
+int mcl_zslab_init(mcl_engine *e, int nz_global, int z_offset, int periodic_z, long long *plane_floats);
+int mcl_zslab_pass(mcl_engine *e, int colour, int measure);
+int mcl_zslab_pack(mcl_engine *e, float *send_lo, float *send_hi);          /* null: skip that side */
+int mcl_zslab_unpack(mcl_engine *e, const float *recv_lo, const float *recv_hi); /* null: no neighbour there */
+int mcl_zslab_sums(mcl_engine *e, int measure, double *d_sums);
+int mcl_zslab_finalize(mcl_engine *e, const double *d_sums, int measure);
 /* With enable != 0, mcl_sweeps replays a captured CUDA graph of two fused sweeps (captured at the first call, again
  * after the plan, the series buffer or the test hooks change) instead of launching kernels one by one; results are
  * identical. Profiling (mcl_profile) uses direct launches. */

@@ -104,6 +104,12 @@ def lib():
             "mcl_local_order": [vp, i, vp],
             "mcl_set_graphs": [vp, i],
             "mcl_set_plan": [vp, i, i],
+            "mcl_zslab_init": [vp, i, i, i, P(ctypes.c_longlong)],
+            "mcl_zslab_pass": [vp, i, i],
+            "mcl_zslab_pack": [vp, vp, vp],
+            "mcl_zslab_unpack": [vp, vp, vp],
+            "mcl_zslab_sums": [vp, i, vp],
+            "mcl_zslab_finalize": [vp, vp, i],
             "mcl_get_plan": [vp, P(CTuning)],
             "mcl_set_adaptation": [vp, i],
             "mcl_extract_samples": [vp, i, ctypes.c_longlong, ctypes.c_ulonglong, vp, vp],
@@ -355,6 +361,27 @@ class Engine:
         t = CTuning()
         check(lib().mcl_get_plan(self._h, ctypes.byref(t)))
         return {k: getattr(t, k) for k, _ in CTuning._fields_ if not k.startswith("ms_") and k != "candidates"}
+
+    # z-slab of a lattice split over processes (mclics_b200.zslab drives these); pointers are device addresses
+    def zslab_init(self, nz_global, z_offset, periodic_z):
+        n = ctypes.c_longlong(0)
+        check(lib().mcl_zslab_init(self._h, nz_global, z_offset, 1 if periodic_z else 0, ctypes.byref(n)))
+        return n.value
+
+    def zslab_pass(self, colour, measure):
+        check(lib().mcl_zslab_pass(self._h, colour, 1 if measure else 0))
+
+    def zslab_pack(self, send_lo, send_hi):
+        check(lib().mcl_zslab_pack(self._h, send_lo or None, send_hi or None))
+
+    def zslab_unpack(self, recv_lo, recv_hi):
+        check(lib().mcl_zslab_unpack(self._h, recv_lo or None, recv_hi or None))
+
+    def zslab_sums(self, measure, d_sums):
+        check(lib().mcl_zslab_sums(self._h, 1 if measure else 0, d_sums))
+
+    def zslab_finalize(self, d_sums, measure):
+        check(lib().mcl_zslab_finalize(self._h, d_sums, 1 if measure else 0))
 
     def set_graphs(self, on=True):
         check(lib().mcl_set_graphs(self._h, 1 if on else 0))

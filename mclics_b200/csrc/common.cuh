@@ -56,6 +56,10 @@ struct RepDesc {
   long long site_off;  // offset of this replica in the unpadded per-site arrays (pt, normals, decisions)
   unsigned long long seed;
   double n_valid;
+  // z-slab of a larger lattice (mcl_zslab_init): local planes 0 and nz - 1 are halo copies of the neighbours'
+  // boundary planes, planes 1 .. nz - 2 are owned; local plane p is global plane zoff + p of a lattice of nzg
+  // planes. Otherwise zslab = 0, zoff = 0, nzg = nz.
+  int zslab, zoff, nzg;
 };
 
 // Mutable per-replica state (device memory).
@@ -71,6 +75,9 @@ struct ObsRecord {
 };
 // Per-block partial sums of the observables: energy, q[6], nsum[3].
 constexpr int kPartials = 10;
+// Per-replica sums a z-slab process contributes to the reduction over processes: the kPartials observables and
+// the accepted rotations.
+constexpr int kZslabSums = kPartials + 1;
 
 __host__ __device__ inline long long dir_index(const RepDesc &r, int c, int x, int y, int z) {
   return r.off + (long long)c * r.comp + ((long long)z * r.py + (y + GY)) * r.px + (x & 1) * r.hp + (x >> 1) + GH;

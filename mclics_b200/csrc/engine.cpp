@@ -295,6 +295,9 @@ int mcl_create(const mcl_model *model, const mcl_replica *replicas, int n_replic
     soff += N;
     D.seed = R.seed;
     D.n_valid = (double)N;
+    D.zslab = 0;
+    D.zoff = 0;
+    D.nzg = R.nz;
     st[r].T = R.T;
     st[r].elecE = R.elecE;
     st[r].ang_var = R.ang_var;
@@ -541,6 +544,7 @@ int mcl_get_sweep_counter(mcl_engine *e, unsigned long long *sweep) {
 int mcl_sweeps(mcl_engine *e, int n, int measure) {
   if (!e) return fail(MCL_ERR_ARG, "null engine");
   if (n < 0) return fail(MCL_ERR_ARG, "negative sweep count");
+  if (e->zslab) return fail(MCL_ERR_STATE, "mcl_sweeps: a z-slab engine sweeps through the mcl_zslab_* calls");
   if (!e->geometry_set) return fail(MCL_ERR_STATE, "custom geometry: call mcl_set_geometry before sweeping");
   if (n == 0) return MCL_OK;
   int rc;
@@ -689,6 +693,7 @@ int mcl_measure(mcl_engine *e, int replica, mcl_observables *out) {
   int rc = check_rep(e, replica, false);
   if (rc) return rc;
   if (!out) return fail(MCL_ERR_ARG, "null output");
+  if (e->zslab) return fail(MCL_ERR_STATE, "mcl_measure: a z-slab engine holds part of a lattice (use mcl_zslab_sums)");
   LaunchCtx c = e->ctx();
   CK(launch_observe(c, e->geo, e->sites, e->d_partials));
   CK(launch_finalize(c, e->sites, e->d_partials, 2, e->d_probe, e->d_probe_len, e->d_done));
@@ -726,8 +731,8 @@ int mcl_set_graphs(mcl_engine *e, int enable) {
 int mcl_autotune(mcl_engine *e, int trial_sweeps, mcl_tuning *out) {
   if (!e) return fail(MCL_ERR_ARG, "null engine");
   if (trial_sweeps < 1 || trial_sweeps > 10000) return fail(MCL_ERR_ARG, "mcl_autotune: trial_sweeps outside 1..10000");
-  if (!e->fused || e->record_dec || e->d_mlp)
-    return fail(MCL_ERR_STATE, "mcl_autotune: the engine does not run the fused tiled sweep");
+  if (!e->fused || e->record_dec || e->d_mlp || e->zslab)
+    return fail(MCL_ERR_STATE, "mcl_autotune: the engine does not run the tiled sweep of whole lattices");
   int rc;
   if ((rc = ensure_series(e, e->series_len + trial_sweeps + 1))) return rc;
   CK(cudaStreamSynchronize(e->stream));
@@ -835,6 +840,81 @@ int mcl_get_plan(mcl_engine *e, mcl_tuning *out) {
   out->threads_per_cta = fused_threads(cfg);
   out->planes_per_segment = seg;
   out->work_items = items;
+  return MCL_OK;
+}
+
+// ---- z-slab decomposition of one lattice over several processes ------------------------------------------------
+int mcl_zslab_init(mcl_engine *e, int nz_global, int z_offset, int periodic_z, long long *plane_floats) {
+  if (!e) return fail(MCL_ERR_ARG, "null engine");
+  if (e->zslab) return fail(MCL_ERR_STATE, "mcl_zslab_init: already a z-slab engine");
+  if (!e->fused || e->n_rep != 1 || e->d_mlp || e->record_dec)
+    return fail(MCL_ERR_STATE, "mcl_zslab_init: needs a bulk or slab engine of one replica on the tiled sweep, without a "
+                               "learned proposal or decision recording");
+  RepDesc &D = e->desc[0];
+  if (D.periodic[2]) return fail(MCL_ERR_ARG, "mcl_zslab_init: create the local replica with a free z axis; the global "
+                                              "z boundary is periodic_z");
+  if (D.nz < 3) return fail(MCL_ERR_ARG, "mcl_zslab_init: the local replica needs at least one owned plane and two halos");
+  if (z_offset < 0 || nz_global < 1 || z_offset + D.nz - 2 > nz_global)
+    return fail(MCL_ERR_ARG, "mcl_zslab_init: owned planes %d..%d outside the global 0..%d", z_offset,
+                z_offset + D.nz - 3, nz_global - 1);
+  if (periodic_z && e->geo == GEO_SLAB) return fail(MCL_ERR_ARG, "mcl_zslab_init: the slab geometry has a free z axis");
+  if (periodic_z && nz_global % 2)
+    return fail(MCL_ERR_INPUT, "mcl_zslab_init: a periodic z axis needs an even number of planes (%d)", nz_global);
+  CK(cudaStreamSynchronize(e->stream));
+  int cfg = 0, seg = 0;
+  int rc = fused_get_cfg(e, &cfg, nullptr, &seg, nullptr);
+  if (rc) return rc;
+  D.zslab = 1;
+  D.zoff = z_offset - 1;
+  D.nzg = nz_global;
+  D.periodic[2] = periodic_z ? 1 : 0;
+  D.n_valid = (double)D.nx * D.ny * nz_global;
+  CK(cudaMemcpy(e->d_desc, &D, sizeof D, cudaMemcpyHostToDevice));
+  e->zslab = true;
+  drop_graphs(e);
+  const bool flip = e->model.flip != 0 || e->model.potential == POT_PEAR;
+  if ((rc = fused_set_plan(e, fused_is_pass_plan(e) ? cfg : (flip ? 4 : 2), 0))) return rc;
+  if (plane_floats) *plane_floats = 3ll * D.py * D.px;
+  return MCL_OK;
+}
+
+int mcl_zslab_pack(mcl_engine *e, float *send_lo, float *send_hi) {
+  if (!e || !e->zslab) return fail(MCL_ERR_STATE, "mcl_zslab_pack: not a z-slab engine");
+  int rc = refresh_ghosts(e);  // the planes go out whole, ghost cells included
+  if (rc) return rc;
+  CK(launch_zslab_planes(e->ctx(), e->d_dir[e->cur], send_lo, send_hi, 1));
+  e->launches++;
+  return MCL_OK;
+}
+
+int mcl_zslab_unpack(mcl_engine *e, const float *recv_lo, const float *recv_hi) {
+  if (!e || !e->zslab) return fail(MCL_ERR_STATE, "mcl_zslab_unpack: not a z-slab engine");
+  CK(launch_zslab_planes(e->ctx(), e->d_dir[e->cur], const_cast<float *>(recv_lo), const_cast<float *>(recv_hi), 0));
+  e->launches++;
+  return MCL_OK;
+}
+
+int mcl_zslab_pass(mcl_engine *e, int colour, int measure) {
+  if (!e || !e->zslab) return fail(MCL_ERR_STATE, "mcl_zslab_pass: not a z-slab engine");
+  if (colour != 0 && colour != 1) return fail(MCL_ERR_ARG, "mcl_zslab_pass: colour must be 0 or 1");
+  int rc = refresh_ghosts(e);
+  if (rc) return rc;
+  return fused_pass(e, colour, measure != 0);
+}
+
+int mcl_zslab_sums(mcl_engine *e, int measure, double *d_sums) {
+  if (!e || !e->zslab) return fail(MCL_ERR_STATE, "mcl_zslab_sums: not a z-slab engine");
+  if (!d_sums) return fail(MCL_ERR_ARG, "mcl_zslab_sums: null buffer");
+  return fused_item_sums(e, measure ? 1 : 0, d_sums);
+}
+
+int mcl_zslab_finalize(mcl_engine *e, const double *d_sums, int measure) {
+  if (!e || !e->zslab) return fail(MCL_ERR_STATE, "mcl_zslab_finalize: not a z-slab engine");
+  if (!d_sums) return fail(MCL_ERR_ARG, "mcl_zslab_finalize: null sums");
+  int rc;
+  if (measure && (rc = ensure_series(e, e->series_len + 1))) return rc;
+  if ((rc = fused_finalize_global(e, d_sums, measure ? 1 : 0))) return rc;
+  if (measure) e->series_len++;
   return MCL_OK;
 }
 

@@ -62,6 +62,7 @@ struct mcl_engine {
   mcl::FusedPlan *fused = nullptr;
   cudaStream_t own_stream = nullptr;
   bool profile = false;
+  bool zslab = false;  // replica 0 is a z-slab of a larger lattice (mcl_zslab_init): pass-level API only
   std::vector<cudaEvent_t> ev_pool;  // pairs (start, stop) of timed sweeps
   size_t ev_used = 0;
   double prof_ms = 0;          // time of already-read event pairs

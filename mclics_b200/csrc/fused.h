@@ -32,4 +32,11 @@ void fused_plan_candidates(const mcl_engine *e, std::vector<std::pair<int, int>>
 int fused_threads(int cfg);
 // Kernel launches of one sweep of the current plan, finalisation included (fused: 2, colour passes: 3).
 int fused_launches_per_sweep(const mcl_engine *e);
+// Z-slab support (colour-pass plans only): whether the plan runs colour passes; one colour pass without the
+// finalisation; each replica's sums over its work items (kZslabSums doubles: energy, q[6], sum n[3], accepted
+// rotations; zeros for the observables when measure = 0); the finalisation from such sums reduced over processes.
+bool fused_is_pass_plan(const mcl_engine *e);
+int fused_pass(mcl_engine *e, int colour, bool measure);
+int fused_item_sums(mcl_engine *e, int measure, double *d_sums);
+int fused_finalize_global(mcl_engine *e, const double *d_sums, int measure);
 }  // namespace mcl

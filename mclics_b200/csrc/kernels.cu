@@ -120,20 +120,25 @@ __global__ void __launch_bounds__(kThreads) k_observe(ModelDev m, const RepDesc 
 // adaptation (src/evolve.cpp:211-220; skipped when adapt = 0), optional series record, reset of the acceptance
 // counter. The last
 // block to finish advances the global sweep counter and the series length. measure: 0 none, 1 append to the
-// series, 2 probe (record the current state into series[rep]; no adaptation, counters untouched).
+// series, 2 probe (record the current state into series[rep]; no adaptation, counters untouched). gsums (z-slab
+// processes): the observables and accepted rotations already summed over all processes (kZslabSums per replica)
+// replace the local partials and the local acceptance counter.
 __global__ void __launch_bounds__(kThreads) k_finalize(const RepDesc *__restrict__ reps, RepState *__restrict__ st,
                                                        const int *__restrict__ obs_first,
                                                        const double *__restrict__ partials, int measure,
                                                        ObsRecord *__restrict__ series, int *__restrict__ series_len,
                                                        unsigned long long *__restrict__ sweep_ctr,
                                                        unsigned int *__restrict__ done_ctr, int n_replicas,
-                                                       int adapt) {
+                                                       int adapt, const double *__restrict__ gsums) {
   const int rep = blockIdx.x;
   __shared__ double red[kThreads / 32][kPartials];
   __shared__ double tot[kPartials];
   const unsigned long long sweep = *sweep_ctr;
   const int slen = *series_len;
-  if (measure) {
+  if (measure && gsums) {
+    if (threadIdx.x < kPartials) tot[threadIdx.x] = gsums[(long long)rep * kZslabSums + threadIdx.x];
+    __syncthreads();
+  } else if (measure) {
     double acc[kPartials];
 #pragma unroll
     for (int k = 0; k < kPartials; k++) acc[k] = 0.0;
@@ -161,13 +166,14 @@ __global__ void __launch_bounds__(kThreads) k_finalize(const RepDesc *__restrict
     const bool probe = measure == 2;  // measurement of the current state only: no adaptation, no counters
     double a = S.pad;
     float av = S.ang_var;
+    const double nacc = gsums ? gsums[(long long)rep * kZslabSums + kPartials] : (double)S.acc;
     if (!probe) {
-      a = (double)S.acc / nv;
+      a = nacc / nv;
       if (!adapt) {
-      } else if (1.0 * (double)S.acc / nv < 0.5) {
+      } else if (1.0 * nacc / nv < 0.5) {
         av = (float)((double)av * 0.99);
         if (av < 0.01) av = 0.01f;
-      } else if (1.0 * (double)S.acc / nv > 0.5) {
+      } else if (1.0 * nacc / nv > 0.5) {
         av = (float)((double)av / 0.99);
         if (av > 1.0) av -= 0.5f;
       }
@@ -326,9 +332,72 @@ cudaError_t launch_observe(const LaunchCtx &c, int geo, const BlockTable &sites,
 }
 
 cudaError_t launch_finalize(const LaunchCtx &c, const BlockTable &sites, const double *partials, int measure,
-                            ObsRecord *series, int *series_len, unsigned int *done_ctr) {
+                            ObsRecord *series, int *series_len, unsigned int *done_ctr, const double *gsums) {
   k_finalize<<<c.n_replicas, kThreads, 0, c.stream>>>(c.reps, c.state, sites.first, partials, measure, series,
-                                                       series_len, c.sweep_ctr, done_ctr, c.n_replicas, c.adapt);
+                                                       series_len, c.sweep_ctr, done_ctr, c.n_replicas, c.adapt,
+                                                       gsums);
+  return cudaGetLastError();
+}
+
+// One block per replica: the replica's partials summed over its blocks (the order k_finalize uses; zeros when
+// measure = 0) and its accepted rotations, kZslabSums doubles per replica.
+__global__ void __launch_bounds__(kThreads) k_item_sums(const RepState *__restrict__ st,
+                                                        const int *__restrict__ obs_first,
+                                                        const double *__restrict__ partials, int measure,
+                                                        double *__restrict__ out) {
+  const int rep = blockIdx.x;
+  __shared__ double red[kThreads / 32][kPartials];
+  double acc[kPartials];
+#pragma unroll
+  for (int k = 0; k < kPartials; k++) acc[k] = 0.0;
+  if (measure)
+    for (int b = obs_first[rep] + threadIdx.x; b < obs_first[rep + 1]; b += kThreads)
+#pragma unroll
+      for (int k = 0; k < kPartials; k++) acc[k] += partials[(long long)b * kPartials + k];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < kPartials; k++) {
+    double v = warp_sum_d(acc[k]);
+    if (lane == 0) red[warp][k] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < kPartials) {
+    double v = 0.0;
+    for (int w = 0; w < kThreads / 32; w++) v += red[w][threadIdx.x];
+    out[(long long)rep * kZslabSums + threadIdx.x] = v;
+  }
+  if (threadIdx.x == 0) out[(long long)rep * kZslabSums + kPartials] = (double)st[rep].acc;
+}
+
+cudaError_t launch_item_sums(const LaunchCtx &c, const BlockTable &items, const double *partials, int measure,
+                             double *out) {
+  k_item_sums<<<c.n_replicas, kThreads, 0, c.stream>>>(c.state, items.first, partials, measure, out);
+  return cudaGetLastError();
+}
+
+// Boundary planes of a z-slab (replica 0) to or from the caller's plane buffers, each [component][py * px] (the
+// whole padded plane, ghost cells included). pack: owned planes 1 and nz - 2 -> lo, hi; unpack: lo, hi -> halo
+// planes 0 and nz - 1. A null buffer skips its side. blockIdx.y selects the side.
+__global__ void k_zslab_planes(const RepDesc *__restrict__ reps, float *__restrict__ dir, float *lo, float *hi,
+                               int pack) {
+  const RepDesc R = reps[0];
+  const long long pf = (long long)R.py * R.px;
+  float *buf = blockIdx.y ? hi : lo;
+  if (!buf) return;
+  const int plane = pack ? (blockIdx.y ? R.nz - 2 : 1) : (blockIdx.y ? R.nz - 1 : 0);
+  float *base = dir + R.off + plane * pf;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < 3 * pf;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long q = i / pf, o = i - q * pf;
+    if (pack)
+      buf[i] = base[q * R.comp + o];
+    else
+      base[q * R.comp + o] = buf[i];
+  }
+}
+
+cudaError_t launch_zslab_planes(const LaunchCtx &c, float *dir, float *lo, float *hi, int pack) {
+  k_zslab_planes<<<dim3(148, 2), kThreads, 0, c.stream>>>(c.reps, dir, lo, hi, pack);
   return cudaGetLastError();
 }
 

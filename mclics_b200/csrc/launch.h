@@ -37,9 +37,17 @@ cudaError_t launch_sweep_checker2_simple(const LaunchCtx &c, int geo, const Bloc
 cudaError_t launch_sweep_ref8(const LaunchCtx &c, int geo, const BlockTable &boxes);
 // Observables of the current state into partials[block][kPartials].
 cudaError_t launch_observe(const LaunchCtx &c, int geo, const BlockTable &sites, double *partials);
-// Per-replica reduction of the partials, S by Jacobi, ang_var adaptation, series record, counter advance.
+// Boundary planes of a z-slab to (pack = 1: owned planes 1, nz - 2) or from (pack = 0: halo planes 0, nz - 1) the
+// caller's buffers of 3 py px floats each; a null buffer skips its side.
+cudaError_t launch_zslab_planes(const LaunchCtx &c, float *dir, float *lo, float *hi, int pack);
+// Per-replica sums of the partials over a block table and the accepted rotations (kZslabSums doubles each).
+cudaError_t launch_item_sums(const LaunchCtx &c, const BlockTable &items, const double *partials, int measure,
+                             double *out);
+// Per-replica reduction of the partials, S by Jacobi, ang_var adaptation, series record, counter advance; with
+// gsums, from sums already reduced over z-slab processes instead of the local partials and acceptance counter.
 cudaError_t launch_finalize(const LaunchCtx &c, const BlockTable &sites, const double *partials, int measure,
-                            ObsRecord *series, int *series_len, unsigned int *done_ctr);
+                            ObsRecord *series, int *series_len, unsigned int *done_ctr,
+                            const double *gsums = nullptr);
 // Periodic ghost cells (x then y) of every replica.
 cudaError_t launch_refresh_ghosts(const LaunchCtx &c, int max_ny_nz, int max_px_nz);
 // One sweep with the learned proposal (two colours, in place); mlp: weights in device layout (learned.cu). With

@@ -901,6 +901,7 @@ extern "C" {
 
 int mcl_set_proposal(mcl_engine *e, const mcl_mlp *mlp, float kappa_max) {
   if (!e) return fail(MCL_ERR_ARG, "null engine");
+  if (mlp && e->zslab) return fail(MCL_ERR_STATE, "mcl_set_proposal: a z-slab engine runs the plain proposal only");
   CKL(cudaStreamSynchronize(e->stream));
   if (!mlp) {
     if (e->d_mlp) cudaFree(e->d_mlp);

@@ -137,9 +137,10 @@ static int build_items(mcl_engine *e, FusedPlan *P) {
   for (int r = 0; r < e->n_rep; r++) {
     first.push_back((int)items.size());
     const RepDesc &D = e->desc[r];
-    for (int z0 = 0; z0 < D.nz; z0 += P->seg)
+    const int zlo = D.zslab ? 1 : 0, zhi = D.zslab ? D.nz - 1 : D.nz;  // a z-slab's halo planes are not swept
+    for (int z0 = zlo; z0 < zhi; z0 += P->seg)
       for (int y0 = 0; y0 < D.ny; y0 += P->ty)
-        for (int x0 = 0; x0 < D.nx; x0 += P->tx) items.push_back(FusedItem{r, x0, y0, z0, std::min(D.nz, z0 + P->seg)});
+        for (int x0 = 0; x0 < D.nx; x0 += P->tx) items.push_back(FusedItem{r, x0, y0, z0, std::min(zhi, z0 + P->seg)});
   }
   first.push_back((int)items.size());
   P->n_items = (int)items.size();
@@ -177,6 +178,8 @@ int fused_set_cfg(mcl_engine *e, int cfg) {
 int fused_set_plan(mcl_engine *e, int cfg, int seg) {
   if (!e->fused) return fail(MCL_ERR_STATE, "this engine does not use the fused tiled sweep");
   if (cfg < 0 || cfg >= kNumCfgs) return fail(MCL_ERR_ARG, "tile configuration %d outside 0..%d", cfg, kNumCfgs - 1);
+  if (kCfgs[cfg].kind == 0 && e->zslab)
+    return fail(MCL_ERR_STATE, "a z-slab engine runs the colour passes (tile configurations 2-%d)", kNumCfgs - 1);
   CKF(cudaStreamSynchronize(e->stream));
   e->fused->cfg = cfg;
   e->fused->seg_override = std::max(0, seg);
@@ -303,6 +306,51 @@ int fused_sweep(mcl_engine *e, bool measure, cudaEvent_t ev0, cudaEvent_t ev1) {
   t.first = P->d_first;
   LaunchCtx c = e->ctx();
   CKF(launch_finalize(c, t, P->d_partials, measure ? 1 : 0, e->d_series, e->d_series_len, e->d_done));
+  return MCL_OK;
+}
+
+bool fused_is_pass_plan(const mcl_engine *e) { return e->fused && kCfgs[e->fused->cfg].kind == 1; }
+
+int fused_pass(mcl_engine *e, int colour, bool measure) {
+  FusedPlan *P = e->fused;
+  if (!P || kCfgs[P->cfg].kind != 1) return fail(MCL_ERR_STATE, "single colour passes need a colour-pass plan");
+  FusedArgs a;
+  a.tmaps = P->d_tmaps;
+  a.out = e->d_dir[e->cur];
+  a.reps = e->d_desc;
+  a.st = e->d_state;
+  a.items = P->d_items;
+  a.partials = P->d_partials;
+  a.sweep_ctr = e->d_sweep;
+  a.err = P->d_err;
+  a.cur = e->cur;
+  a.measure = measure && colour == 1 ? 1 : 0;
+  a.timeout_ns = P->timeout_ns;
+  a.skip_first_load = P->skip_first_load;
+  a.colour = colour;
+  const cudaError_t err = dispatch(e, a, launch_desc(e, P));
+  if (err != cudaSuccess) return cuda_fail(err, "colour pass launch");
+  e->launches += 1;
+  return MCL_OK;
+}
+
+int fused_item_sums(mcl_engine *e, int measure, double *d_sums) {
+  FusedPlan *P = e->fused;
+  if (!P) return fail(MCL_ERR_STATE, "this engine does not use the tiled sweep");
+  BlockTable t;
+  t.first = P->d_first;
+  CKF(launch_item_sums(e->ctx(), t, P->d_partials, measure, d_sums));
+  e->launches += 1;
+  return MCL_OK;
+}
+
+int fused_finalize_global(mcl_engine *e, const double *d_sums, int measure) {
+  FusedPlan *P = e->fused;
+  if (!P) return fail(MCL_ERR_STATE, "this engine does not use the tiled sweep");
+  BlockTable t;
+  t.first = P->d_first;
+  CKF(launch_finalize(e->ctx(), t, P->d_partials, measure, e->d_series, e->d_series_len, e->d_done, d_sums));
+  e->launches += 1;
   return MCL_OK;
 }
 

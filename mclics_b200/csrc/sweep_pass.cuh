@@ -119,8 +119,12 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_pass(ModelDev m, FusedArgs a
   __syncthreads();
 
   // Plane p (local index lp = p - pbeg) lives in slot lp % NSLP; every use of a slot completes one barrier phase.
+  // A z-slab's halo planes (local 0 and nz - 1) exist unless they lie beyond a free global boundary; its work items
+  // cover the owned planes only, so no local plane index wraps. zoff = 0, nzg = nz otherwise.
   const int pbeg = z0 - 1, pend = z1;
-  auto plane_exists = [&](int p) { return perz || (p >= 0 && p < nz); };
+  const int zoff = R.zoff, nzg = R.nzg;
+  const int pz_lo = R.zslab ? -zoff : 0, pz_hi = R.zslab ? nzg - zoff : nz;
+  auto plane_exists = [&](int p) { return perz || (p >= pz_lo && p < pz_hi); };
   auto wrapz = [&](int p) { return p < 0 ? p + nz : (p >= nz ? p - nz : p); };
   auto slot_ptr = [&](int p) -> float * { return slots + (size_t)((unsigned)(p - pbeg) % NSLP) * SLOT; };
   int last_issued = pbeg - 1;  // meaningful in thread 0 only
@@ -182,7 +186,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_pass(ModelDev m, FusedArgs a
 #pragma unroll
     for (int q = 0; q < 3; q++) pd[t][q] = make_float2(0.f, 0.f);
     if (ok && live[t] && plane_exists(z0 - 1)) {
-      const float *q0 = slot_ptr(z0 - 1) + ((rr[t] + 1) * 2 + ((colour + y0 + rr[t] + z0) & 1)) * HALF + jb;
+      const float *q0 = slot_ptr(z0 - 1) + ((rr[t] + 1) * 2 + ((colour + y0 + rr[t] + z0 + zoff) & 1)) * HALF + jb;
 #pragma unroll
       for (int q = 0; q < 3; q++) pd[t][q] = *reinterpret_cast<const float2 *>(q0 + q * PF);
     }
@@ -192,7 +196,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_pass(ModelDev m, FusedArgs a
     if (!ok) break;
     if (tid == 0) issue(k + 3);
     if (!live[0]) continue;  // rows grow with t: a dead first row has no live rows after it
-    const int h = (colour + y0 + r0 + k) & 1;
+    const int h = (colour + y0 + r0 + k + zoff) & 1;  // colours follow global planes (zoff: z-slab offset)
     const int x = x0 + 4 * p + h;
     const bool v0 = x < nx, v1 = x + 2 < nx;
     const float *cs_k = slot_ptr(k);
@@ -211,15 +215,16 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_pass(ModelDev m, FusedArgs a
     // of the update costs registers that the 3-CTA configuration does not have; the runtime surface test then
     // makes the site terms zero).
     constexpr bool kNever = GEO == GEO_BULK && !FIELD, kAlways = FIELD || (GEO == GEO_SLAB && TPT == 1);
-    const bool single_terms = kNever ? false : (kAlways ? true : (k == 0 || k == nz - 1));
+    const bool single_terms = kNever ? false : (kAlways ? true : (k + zoff == 0 || k + zoff == nzg - 1));
     auto step = [&](auto single_tag) {
       constexpr bool SINGLE = decltype(single_tag)::value;
       const bool has_below = plane_exists(k - 1);
       const float *above = plane_exists(k + 1) ? slot_ptr(k + 1) : nullptr;
-      const int zw = k;  // computed planes lie inside the lattice
+      const int zw = k;         // computed planes lie inside the local lattice
+      const int zg = k + zoff;  // and this is their global index (draws, surfaces)
       int sid = -1;
       float sz = 0.f;
-      if (SINGLE && GEO == GEO_SLAB) sid = slab_surface(zw, nz, sz);
+      if (SINGLE && GEO == GEO_SLAB) sid = slab_surface(zg, nzg, sz);
       const Vec3 sn{0.f, 0.f, sz};
       float2 o[TPT][3];
       SiteResultT<float2> res[TPT];
@@ -243,10 +248,10 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_pass(ModelDev m, FusedArgs a
         }
         Draw d0, d1;
         if (FLIP) {
-          d0 = site_draw(c.seed, c.sweep, x, y, zw, nx, ny, true);
-          d1 = site_draw(c.seed, c.sweep, x + 2, y, zw, nx, ny, true);
+          d0 = site_draw(c.seed, c.sweep, x, y, zg, nx, ny, true);
+          d1 = site_draw(c.seed, c.sweep, x + 2, y, zg, nx, ny, true);
         } else {  // one Philox call serves both sites (x & ~2 is shared: x % 4 = h)
-          const U4 out = site_draws(c.seed, c.sweep, pair_counter(x, y, zw, nx, ny), 0);
+          const U4 out = site_draws(c.seed, c.sweep, pair_counter(x, y, zg, nx, ny), 0);
           d0 = pair_half(out, 0u);
           d1 = pair_half(out, 1u);
         }
