@@ -339,6 +339,76 @@ def gpu_arm(args, rank, world, local_rank):
                 acc=float(rec["acceptance"]), cfg=cfg, tuning=tuning)
 
 
+def zslab_arm(args, rank, world, local_rank):
+    """The workload's first lattice split along z over the ranks (mclics_b200.zslab): every rank sweeps its planes
+    with the colour passes and exchanges its boundary planes after each pass (NCCL send/recv through
+    torch.distributed), one FP64 all-reduce of the sums per sweep. Strong scaling: the lattice is the same for
+    every N. Device time of K measured sweeps, max over ranks."""
+    import torch
+    from mclics_b200 import zslab
+    torch.cuda.set_device(local_rank)
+    model, reps, cfg, ic = workload(args.workload)
+    r0 = reps[0]
+    nx, ny, nz = r0["nx"], r0["ny"], r0["nz"]
+    per, geo = r0.get("periodic", (1, 1, 1)), r0.get("geometry", "bulk")
+    slab = zslab.ZSlab(model, nx, ny, nz, rank, world, zslab.TorchExchange(), geometry=geo, periodic_xy=per[:2],
+                       periodic_z=bool(per[2]) and geo != "slab", T=r0["T"], seed=r0["seed"])
+    slab.upload_global(initial_state(nx * ny * nz, ic, SEED))  # the same global lattice on every rank
+    slab.sweeps(args.warmup, measure=True)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(slab.stream)
+    slab.sweeps(args.steps, measure=True)
+    e1.record(slab.stream)
+    e1.synchronize()
+    clocks.stop()
+    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    rec = slab.series()[-1]
+    out = dict(dev_ms=float(t[0]), sites=nx * ny * nz, nz_own=slab.nz_own, cfg=cfg, clocks=clocks.summary(),
+               plan=slab.eng.plan(), S=float(rec["S"]), E=float(rec["energy"]), acc=float(rec["acceptance"]))
+    slab.eng.close()
+    return out
+
+
+def zslab_main(args, rank, world, local_rank):
+    import torch
+    if world > 1:
+        torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    res = zslab_arm(args, rank, world, local_rank)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return 0
+    peak, peak_kind = measured_peaks()
+    sec = res["dev_ms"] / 1e3
+    achieved = res["sites"] * BYTES_PER_SITE_UPDATE * args.steps / sec / world / 1e9  # per GPU
+    config = dict(res["cfg"], step="1 sweep + measurement of the whole lattice",
+                  parallelism="one lattice split along z over %d GPUs (%d planes on rank 0)" % (world, res["nz_own"]),
+                  decomposition="z-slab: boundary planes exchanged after each colour pass, 11-double all-reduce "
+                                "per sweep", plan=res["plan"], global_sites_per_step=res["sites"])
+    line = {
+        "metric": METRIC, "value": res["sites"] * args.steps / sec, "unit": "site-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["dev_ms"] / args.steps,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": config, "mode": "zslab",
+        "e2e": None, "e2e_note": "device-timed only: the z-slab mode measures the decomposition, not host transfers",
+        "gpu_launches": 8 * args.steps,  # per sweep: 2 passes, 2 packs, 2 unpacks, sums, finalisation
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "traffic": None, "per": "GPU"},
+        "clocks": res["clocks"],
+        "physics": {"S_last": res["S"], "E_last": res["E"], "acceptance_last": res["acc"]},
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def learned_compare(args):
     """Learned vs plain proposal on one workload (c4: LL 128^3 at T = 0.3, 0.8, 1.12): the network is trained on
     the GPU from plain-sweep states (seed 3), then both proposals run the same number of measured sweeps from the
@@ -448,6 +518,8 @@ def main():
     ap.add_argument("--therm-sweeps", type=int, default=5000,
                     help="--learned: plain sweeps from the ordered start before both arms are measured")
     ap.add_argument("--train-samples", type=int, default=10_000_000)
+    ap.add_argument("--zslab", action="store_true",
+                    help="one lattice of the workload split along z over the N ranks (strong scaling)")
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"],
                     help="c2 (default): the headline GHRL 256^3 slab; others: the remaining configurations")
     args = ap.parse_args()
@@ -460,6 +532,8 @@ def main():
         if rank != 0:
             return 0
         return learned_compare(args)
+    if args.zslab and args.impl != "reference":
+        return zslab_main(args, rank, world, local_rank)
     _, _, config, _ = workload(args.workload) if args.impl != "reference" else workload("c2")
     config = dict(config, step="1 sweep + measurement of every lattice", accumulators="f64 (energy, Q, sum n)",
                   parallelism=("replicas split across %d GPUs" % args.gpus if args.shard and args.gpus > 1
