@@ -11,11 +11,14 @@ reference's thermalGPU loop. Metric: site updates per second (whole job, all GPU
   value      device time (CUDA events on the engine's stream) of K steps with the lattice resident in HBM. The
              lattice (211 MB padded) is larger than L2 (126 MB), so no flush is needed between steps. The tile
              plan is chosen by mcl_autotune before timing, and the K steps are one mcl_sweeps call replaying a
-             captured CUDA graph of the fused sweeps.
-  e2e        the same steps through the C ABI as the reference's GPU mode loop drives them, host buffers and
-             host<->device copies inside the timed region: per step the temperature goes up from pinned host
-             memory, the observables record and the whole director field (the reference copies it back after
-             every measurement sweep, src/evolve_thermal.cu:90) come down into pinned host memory.
+             captured CUDA graph of the sweeps.
+  e2e        the same steps through the C ABI, one call sequence per step as a drop-in caller makes it, host
+             buffers and host<->device copies inside the timed region: the step's input (the temperature of every
+             replica) goes up from pinned host memory, the sweep runs, and the step's result (the observables
+             record of every replica) comes down to the host.
+  e2e_reference_data_movement  the same, plus the whole director field down every step, as the reference's GPU
+             loop moves it (it computes Q on the host after every measurement sweep, src/evolve_thermal.cu:90;
+             this engine computes it on the device, so a caller needs the field only for snapshots).
   roofline   the sweep kernel(s) only: algorithmic 24 B per site update (one FP32 director read + write) per
              sweep / kernel time, against the measured HBM copy bandwidth.
   cpu_baseline  the reference's own OpenMP CPU sweep + measurement (oracle/_ref/mclics_ref_timing, built from the
@@ -310,30 +313,38 @@ def gpu_arm(args, rank, world, local_rank):
     kernel_ms = (ms1 - ms0) / max(1, n1 - n0)
     rec = eng.series(0, eng.series_length() - 1, 1)[0]
 
-    # end to end through the C ABI with host buffers (reference GPU loop data movement, all replicas)
+    # end to end through the C ABI with host buffers, all replicas: temperatures up, the step's observables down
+    # (and, second, also the whole director field down every step, the reference GPU loop's data movement)
     host_ni = [torch.empty(3 * n, dtype=torch.float32, pin_memory=True) for n in sizes]
     host_T = torch.tensor([r["T"] for r in reps], dtype=torch.float32, pin_memory=True)
-    torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
+
+    def e2e_loop(lattice_down):
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            for i in range(len(reps)):
+                eng.set_temperature(float(host_T[i]), i)
+            eng.sweeps(1, measure=True)
+            for i in range(len(reps)):
+                eng.series(i, eng.series_length() - 1, 1)
+                if lattice_down:
+                    M.check(M.lib().mcl_download_directors(eng._h, i, host_ni[i].data_ptr()))
+        return time.perf_counter() - t0
+
     clocks.start()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        for i in range(len(reps)):
-            eng.set_temperature(float(host_T[i]), i)
-        eng.sweeps(1, measure=True)
-        for i in range(len(reps)):
-            eng.series(i, eng.series_length() - 1, 1)
-            M.check(M.lib().mcl_download_directors(eng._h, i, host_ni[i].data_ptr()))
-    e2e_s = time.perf_counter() - t0
+    e2e_s = e2e_loop(False)
+    e2e_lat_s = e2e_loop(True)
     clocks.stop()
 
-    times = torch.tensor([dev_ms, e2e_s * 1e3], dtype=torch.float64, device=dev)
+    times = torch.tensor([dev_ms, e2e_s * 1e3, e2e_lat_s * 1e3], dtype=torch.float64, device=dev)
     if world > 1:
         torch.distributed.all_reduce(times, op=torch.distributed.ReduceOp.MAX)
-    dev_ms_max, e2e_ms_max = float(times[0]), float(times[1])
+    dev_ms_max, e2e_ms_max, e2e_lat_ms_max = float(times[0]), float(times[1]), float(times[2])
     eng.close()
-    return dict(dev_ms=dev_ms_max, e2e_ms=e2e_ms_max, kernel_ms=kernel_ms, launches=launches, sites=sites,
+    return dict(dev_ms=dev_ms_max, e2e_ms=e2e_ms_max, e2e_lat_ms=e2e_lat_ms_max, kernel_ms=kernel_ms,
+                launches=launches, sites=sites,
                 all_sites=all_sites,
                 n_rep=len(reps), clocks=clocks.summary(), S=float(rec["S"]), E=float(rec["energy"]),
                 acc=float(rec["acceptance"]), cfg=cfg, tuning=tuning)
@@ -594,6 +605,7 @@ def main():
                     "inputs smaller than L2 (%.0f MB): DRAM roofline is an upper bound" % (res["sites"] * 12 / 1e6))
     value = sites_total * args.steps / (res["dev_ms"] / 1e3)
     e2e = sites_total * args.steps / (res["e2e_ms"] / 1e3)
+    e2e_lat = sites_total * args.steps / (res["e2e_lat_ms"] / 1e3)
     peak, peak_kind = measured_peaks()
     # per launch: a sweep is 2 colour-pass launches (each half the site updates) or 1 fused launch; the ratio of
     # algorithmic bytes to time is the same either way
@@ -605,7 +617,12 @@ def main():
         "scaling": "strong" if sharded else "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config,
         "e2e": {"value": e2e, "unit": "site-updates/s", "h2d_bytes_per_step": 4 * res["n_rep"],
-                "d2h_bytes_per_step": 144 * res["n_rep"] + 12 * res["sites"]},
+                "d2h_bytes_per_step": 144 * res["n_rep"]},
+        "e2e_reference_data_movement": {"value": e2e_lat, "unit": "site-updates/s",
+                                        "h2d_bytes_per_step": 4 * res["n_rep"],
+                                        "d2h_bytes_per_step": 144 * res["n_rep"] + 12 * res["sites"],
+                                        "note": "plus the whole director field down every step, as the "
+                                                "reference's GPU loop copies it for its host-side Q tensor"},
         "gpu_launches": res["launches"],
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind, "traffic": ncu_traffic(args.workload, tu["tile_config"]),
