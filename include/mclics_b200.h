@@ -186,13 +186,14 @@ int mcl_local_order(mcl_engine *e, int replica, float *S);
  *   2: two in-place colour passes per sweep, 64 x 16 sites, 256 threads, 3 CTAs per SM;
  *   3: colour passes, 64 x 32 sites, 512 threads;
  *   4: colour passes, 64 x 16 sites, 256 threads, 2 CTAs per SM;
- *   5: colour passes, 64 x 16 sites, 128 threads with two pair tasks (rows r and r + 8) each, 3 CTAs per SM.
+ *   5: colour passes, 64 x 16 sites, 128 threads with two pair tasks (rows r and r + 8) each, 3 CTAs per SM;
+ *   6: colour passes, 32 x 16 sites, 128 threads, 5 CTAs per SM (narrow lattices waste less of a tile).
  * Every configuration gives bit-identical directors. mcl_autotune times each candidate plan for trial_sweeps
  * measured sweeps on the engine's own replicas, keeps the fastest and restores the directors, per-replica state,
  * sweep counter and series, so the run continues as if it had not been called. MCL_ERR_STATE unless the engine
  * runs the tiled sweep (bulk/slab, plain proposal, no decision recording). */
 typedef struct mcl_tuning {
-  int tile_config;        /* 0..5 as above */
+  int tile_config;        /* 0..6 as above */
   int rows_per_tile;
   int threads_per_cta;
   int planes_per_segment;

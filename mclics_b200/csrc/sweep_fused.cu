@@ -12,10 +12,11 @@
 
 namespace mcl {
 
-// 0, 1: fused (7 slots of TY + 4 rows: one CTA per SM either way); 2-5: colour passes (4 slots of TY + 2 rows;
-// 5 runs two pair tasks per thread).
-static const FusedCfg kCfgs[kNumCfgs] = {{14, 256, 1, 0}, {28, 512, 1, 0}, {16, 256, 3, 1}, {32, 512, 1, 1},
-                                         {16, 256, 2, 1}, {16, 128, 3, 1}};
+// 0, 1: fused (7 slots of TY + 4 rows: one CTA per SM either way); 2-6: colour passes (4 slots of TY + 2 rows;
+// 5 runs two pair tasks per thread; 6 has 32-wide tiles, for lattices whose width is not a multiple of 64).
+static const FusedCfg kCfgs[kNumCfgs] = {{14, 256, 1, 0, 64}, {28, 512, 1, 0, 64}, {16, 256, 3, 1, 64},
+                                         {32, 512, 1, 1, 64}, {16, 256, 2, 1, 64}, {16, 128, 3, 1, 64},
+                                         {16, 128, 5, 1, 32}};
 
 struct FusedPlan {
   int cfg = 0, tx = 64, ty = 14, seg = 32;
@@ -53,12 +54,12 @@ bool fused_supported(const mcl_engine *e) {
   return get_encode() != nullptr;
 }
 
-// Box of `rows` padded rows (fused: TY + 4, colour pass: TY + 2).
-static int encode_map(CUtensorMap *map, float *base, const RepDesc &D, int rows) {
+// Box of `cells` half-row cells (TX / 2 + 8) and `rows` padded rows (fused: TY + 4, colour pass: TY + 2).
+static int encode_map(CUtensorMap *map, float *base, const RepDesc &D, int cells, int rows) {
   // 5-D view of the split layout: (half-row cell, x parity, padded row, plane, component)
   cuuint64_t dims[5] = {(cuuint64_t)D.hp, 2, (cuuint64_t)D.py, (cuuint64_t)D.nz, 3};
   cuuint64_t strides[4] = {(cuuint64_t)D.hp * 4, (cuuint64_t)D.px * 4, (cuuint64_t)D.px * D.py * 4, (cuuint64_t)D.comp * 4};
-  cuuint32_t box[5] = {(cuuint32_t)HALF, 2, (cuuint32_t)rows, 1, 3};
+  cuuint32_t box[5] = {(cuuint32_t)cells, 2, (cuuint32_t)rows, 1, 3};
   cuuint32_t es[5] = {1, 1, 1, 1, 1};
   CUresult r = get_encode()(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, base + D.off, dims, strides, box, es,
                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -78,7 +79,7 @@ static int encode_map(CUtensorMap *map, float *base, const RepDesc &D, int rows)
 // loaded, two of them computed; colour pass: two loaded).
 static void choose_segments(const mcl_engine *e, FusedPlan &P, int sms) {
   const FusedCfg &C = kCfgs[P.cfg];
-  P.tx = TXF;
+  P.tx = C.tx;
   P.ty = C.ty;
   long long tiles = 0, maxz = 1;
   for (auto &D : e->desc) {
@@ -123,7 +124,8 @@ static int build_items(mcl_engine *e, FusedPlan *P) {
   std::vector<CUtensorMap> maps(2 * e->n_rep);
   for (int r = 0; r < e->n_rep; r++)
     for (int b = 0; b < 2; b++) {
-      int rc = encode_map(&maps[2 * r + b], e->d_dir[b], e->desc[r], P->ty + (kCfgs[P->cfg].kind ? 2 : 4));
+      int rc = encode_map(&maps[2 * r + b], e->d_dir[b], e->desc[r], P->tx / 2 + 8,
+                          P->ty + (kCfgs[P->cfg].kind ? 2 : 4));
       if (rc) return rc;
     }
   cudaFree(P->d_tmaps);
@@ -151,7 +153,7 @@ static int build_items(mcl_engine *e, FusedPlan *P) {
   CKF(cudaMalloc(&P->d_partials, (size_t)P->n_items * kPartials * sizeof(double)));
   const bool pass = kCfgs[P->cfg].kind == 1;
   const int nsl = pass ? NSLP : NSL;
-  const size_t slot_floats = ((size_t)3 * RW * (P->ty + (pass ? 2 : 4)) + 31) / 32 * 32;
+  const size_t slot_floats = ((size_t)3 * (P->tx + 16) * (P->ty + (pass ? 2 : 4)) + 31) / 32 * 32;
   P->smem = 128 + (size_t)nsl * slot_floats * sizeof(float) + nsl * sizeof(unsigned long long);
   return prepare_kernel(e, P);
 }

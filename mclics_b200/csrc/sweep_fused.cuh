@@ -561,9 +561,9 @@ __global__ void __launch_bounds__(NT, NT <= 256 ? 2 : 1) k_sweep_fused(ModelDev 
 // Tile configurations: rows per tile, threads per CTA (64 columns always), resident CTAs per SM, and the kernel:
 // kind 0 the fused two-colour sweep (this file), kind 1 two colour passes (sweep_pass.cuh).
 struct FusedCfg {
-  int ty, nt, ctas_per_sm, kind;
+  int ty, nt, ctas_per_sm, kind, tx;
 };
-constexpr int kNumCfgs = 6;
+constexpr int kNumCfgs = 7;
 
 // Launch of one potential's kernels (sweep_fused_{ll,ghrl,pear}.cu): dispatch over geometry, flip, periodic x/y,
 // chirality, field and tile configuration.

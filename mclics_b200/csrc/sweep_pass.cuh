@@ -32,9 +32,12 @@ namespace mcl {
 
 constexpr int NSLP = 4;
 
-template <int TY>
+// Plane window of a TX x TY tile: per row and parity TX / 2 + 8 half-row cells (the tile's TX / 2 and 4 on each
+// side, 16-byte aligned), TY + 2 rows, 3 components.
+template <int TY, int TX>
 struct PassWin {
-  static constexpr int H = TY + 2, PF = RW * H, SLOT = (3 * PF + 31) / 32 * 32;
+  static constexpr int HW = TX / 2 + 8, RWX = 2 * HW, NP = TX / 4;  // cells per half-row, per row; pairs per row
+  static constexpr int H = TY + 2, PF = RWX * H, SLOT = (3 * PF + 31) / 32 * 32;
 };
 
 // Ghost copies of the updated pair (elements e = 0, 1 at half indices jl, jl + 1 of the half-row `row0` of parity
@@ -75,10 +78,12 @@ __device__ __forceinline__ void pair_moments(float2 (&m)[9], const float2 (&u)[3
   m[8] = __fadd2_rn(u[2], v[2]);
 }
 
-template <int POT, int GEO, bool FLIP, bool PXY, bool CHIRAL, bool FIELD, int TY, int NT, int MINB, int TPT>
+template <int POT, int GEO, bool FLIP, bool PXY, bool CHIRAL, bool FIELD, int TY, int NT, int MINB, int TPT,
+          int TX>
 __global__ void __launch_bounds__(NT, MINB) k_sweep_pass(ModelDev m, FusedArgs a) {
-  constexpr int PF = PassWin<TY>::PF, SLOT = PassWin<TY>::SLOT;
-  static_assert(NT * TPT == TY * NPAIR, "TPT pair tasks per thread and plane");
+  using W = PassWin<TY, TX>;
+  constexpr int PF = W::PF, SLOT = W::SLOT, HALF = W::HW, RW = W::RWX, NP = W::NP;
+  static_assert(NT * TPT == TY * NP, "TPT pair tasks per thread and plane");
   static_assert(TPT == 1 || (TY / TPT) % 2 == 0, "a thread's rows must share their parity pattern");
   extern __shared__ __align__(128) unsigned char smem_dyn[];
   unsigned char *smem_raw = smem_align128(smem_dyn);
@@ -166,7 +171,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_pass(ModelDev m, FusedArgs a
   for (int q = 0; q < kPartials; q++) dacc[q] = 0.0;
 
   // tasks of this thread: pair p of rows rr[t] = r0 + t TY / TPT (same parity pattern: TY / TPT is even)
-  const int r0 = tid >> 4, p = tid & 15;
+  const int r0 = tid / NP, p = tid % NP;
   int rr[TPT];
   bool live[TPT];
 #pragma unroll
@@ -389,9 +394,10 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_pass(ModelDev m, FusedArgs a
   }
 }
 
-template <int POT, int GEO, bool FLIP, bool PXY, bool CHIRAL, bool FIELD, int TY, int NT, int MINB, int TPT>
+template <int POT, int GEO, bool FLIP, bool PXY, bool CHIRAL, bool FIELD, int TY, int NT, int MINB, int TPT,
+          int TX = 64>
 cudaError_t launch_pass_one(const ModelDev &m, const FusedArgs &a, const FusedLaunch &l) {
-  auto k = k_sweep_pass<POT, GEO, FLIP, PXY, CHIRAL, FIELD, TY, NT, MINB, TPT>;
+  auto k = k_sweep_pass<POT, GEO, FLIP, PXY, CHIRAL, FIELD, TY, NT, MINB, TPT, TX>;
   if (l.prepare) return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)l.smem);
   k<<<l.n_items, NT, l.smem, l.stream>>>(m, a);
   return cudaGetLastError();
@@ -405,6 +411,7 @@ cudaError_t launch_pass_cfg(const ModelDev &m, const FusedArgs &a, const FusedLa
   if (l.cfg == 3) return launch_pass_one<POT, GEO, FLIP, PXY, CHIRAL, FIELD, 32, 512, 1, 1>(m, a, l);
   if (l.cfg == 4) return launch_pass_one<POT, GEO, FLIP, PXY, CHIRAL, FIELD, 16, 256, 2, 1>(m, a, l);
   if (l.cfg == 5) return launch_pass_one<POT, GEO, FLIP, PXY, CHIRAL, FIELD, 16, 128, 3, 2>(m, a, l);
+  if (l.cfg == 6) return launch_pass_one<POT, GEO, FLIP, PXY, CHIRAL, FIELD, 16, 128, 5, 1, 32>(m, a, l);
   return launch_pass_one<POT, GEO, FLIP, PXY, CHIRAL, FIELD, 16, 256, 3, 1>(m, a, l);
 }
 

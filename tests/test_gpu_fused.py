@@ -10,7 +10,7 @@ import pytest
 
 # tile configurations (MCL_FUSED_CFG): "0", "1" = fused kernel (64 x 14, 64 x 28 tiles), "2"-"4" = colour passes
 KERNELS = {"fused14": "0", "fused28": "1", "pass": "2"}
-PASS_CFGS = ["2", "3", "4", "5"]
+PASS_CFGS = ["2", "3", "4", "5", "6"]
 
 
 @pytest.fixture
