@@ -119,12 +119,24 @@ __device__ __forceinline__ bool tc_try_wait(unsigned long long *bar, unsigned pa
   return ok != 0;
 }
 
+// try_wait with a suspend-time hint: a thread whose phase is not complete sleeps (up to hint_ns) instead of
+// returning at once, so the threads waiting for an MMA stage take no issue slots from the SM's other CTAs.
+__device__ __forceinline__ bool tc_try_wait_sleep(unsigned long long *bar, unsigned parity, unsigned hint_ns) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(tc_smem(bar)), "r"(parity), "r"(hint_ns)
+      : "memory");
+  return ok != 0;
+}
+
 __device__ __forceinline__ bool tc_wait(unsigned long long *bar, unsigned parity, long long timeout_ns) {
   if (tc_try_wait(bar, parity)) return true;
   unsigned long long t0;
   asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t0));
   while (true) {
-    if (tc_try_wait(bar, parity)) return true;
+    if (tc_try_wait_sleep(bar, parity, 20000u)) return true;
     unsigned long long t;
     asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
     if ((long long)(t - t0) > timeout_ns) return false;
