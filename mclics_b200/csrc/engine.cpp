@@ -584,6 +584,21 @@ int mcl_sweeps(mcl_engine *e, int n, int measure) {
     } else {
       LaunchCtx c = e->ctx();
       if (ev0) CK(cudaEventRecord(ev0, e->stream));
+      if (e->d_mlp && e->mlp_tc && e->learned_pass && e->fused) {  // colour passes on streamed planes
+        const LearnedMlp lm{e->d_mlp, e->d_mlp_tc, e->d_lerr, e->mlp_tc};
+        LearnedPassView v;
+        if ((rc = refresh_ghosts(e))) return rc;  // the passes read ghost cells and keep them current
+        if ((rc = fused_learned_view(e, &v))) return rc;
+        CK(launch_learned_pass(c, e->geo, v, lm, e->kappa_max, measure ? 1 : 0, e->d_dir[e->cur], e->cur));
+        e->launches += 2;
+        if (ev1) CK(cudaEventRecord(ev1, e->stream));
+        BlockTable t;
+        t.first = v.first;
+        CK(launch_finalize(c, t, v.partials, measure ? 1 : 0, e->d_series, e->d_series_len, e->d_done));
+        e->launches++;
+        if (measure) e->series_len++;
+        continue;
+      }
       if (e->d_mlp) {  // observables fused into the two colour kernels, finalised over the same block table
         const LearnedMlp lm{e->d_mlp, e->d_mlp_tc, e->d_lerr, e->mlp_tc};
         CK(launch_sweep_learned(c, e->geo, e->half, lm, e->kappa_max, measure ? 1 : 0, e->d_partials));

@@ -72,6 +72,7 @@ struct mcl_engine {
   mcl::MlpTC *d_mlp_tc = nullptr;  // the same weights in the tcgen05 layout
   unsigned *d_lerr = nullptr;      // learned-sweep error word
   bool mlp_tc = true;              // learned sweeps run the network on tcgen05
+  bool learned_pass = true;        // ... as colour passes on streamed planes (bulk/slab with the tiled sweep)
   double *d_xpart = nullptr;   // scratch of mcl_measure_extras (allocated at its first call)
   float kappa_max = 500.f;
   bool adapt = true;           // ang_var adaptation after each sweep (the reference's behaviour)

@@ -37,6 +37,9 @@ int fused_launches_per_sweep(const mcl_engine *e);
 // finalisation; each replica's sums over its work items (kZslabSums doubles: energy, q[6], sum n[3], accepted
 // rotations; zeros for the observables when measure = 0); the finalisation from such sums reduced over processes.
 bool fused_is_pass_plan(const mcl_engine *e);
+// Work items, tensor maps and partials of the learned colour passes' own plan (64 x 8 tiles), built at the first
+// call; MCL_ERR_STATE without the tiled sweep.
+int fused_learned_view(mcl_engine *e, LearnedPassView *v);
 int fused_pass(mcl_engine *e, int colour, bool measure);
 int fused_item_sums(mcl_engine *e, int measure, double *d_sums);
 int fused_finalize_global(mcl_engine *e, const double *d_sums, int measure);

@@ -1,11 +1,14 @@
 // Host-side launchers of the device kernels (implemented in the .cu files, used by engine.cpp).
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include "common.cuh"
 
 namespace mcl {
+
+struct FusedItem;
 
 // Block work table: block b of a launch works on replica rep[b], items [base[b], base[b] + blockDim).
 struct BlockTable {
@@ -61,6 +64,18 @@ struct LearnedMlp {
   unsigned *err;       // error word (tensor-core timeout)
   bool use_tc;
 };
+// The learned sweep as two in-place colour passes on TMA-streamed planes (bulk and slab, tcgen05 network): the
+// work items, tensor maps and per-item partials of a 64 x 8-tile plan (fused_learned_view); finalise with
+// launch_finalize over `first` and `partials`.
+struct LearnedPassView {
+  const CUtensorMap *tmaps = nullptr;
+  const FusedItem *items = nullptr;
+  int n_items = 0;
+  double *partials = nullptr;
+  int *first = nullptr;
+};
+cudaError_t launch_learned_pass(const LaunchCtx &c, int geo, const LearnedPassView &v, const LearnedMlp &mlp,
+                                float kappa_max, int measure, float *dir, int cur);
 cudaError_t launch_sweep_learned(const LaunchCtx &c, int geo, const BlockTable &half, const LearnedMlp &mlp,
                                  float kappa_max, int measure, double *partials);
 // AoS (reference layout) <-> padded SoA for one replica.

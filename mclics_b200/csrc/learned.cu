@@ -31,6 +31,7 @@
 #include "common.cuh"
 #include "engine.h"
 #include "launch.h"
+#include "sweep_fused.cuh"
 #include "mlp_tc.cuh"
 #include "physics.cuh"
 #include "site_access.cuh"
@@ -806,6 +807,285 @@ __global__ void k_round(const float *__restrict__ params, float *__restrict__ wr
   if (p < kNP) wr[p] = pass_value(p, params[p]);
 }
 
+// ---- the learned sweep as colour passes on TMA-streamed planes (bulk and slab, tcgen05) -------------------------
+// The plain colour pass (sweep_pass.cuh) with the learned proposal: work item = (replica, 64 x 8 tile, z segment);
+// per plane the tile holds exactly 256 sites of the colour, one per thread (warp w: row y0 + w, all of one x
+// parity), so each plane step is one 256-row tcgen05 MLP batch (cta_mlp_tc). Neighbours come from the plane
+// window in shared memory (4 slots, two planes in flight, the -z neighbour carried from the step before), the
+// update is written in place with the ghost copies of edge sites, and every per-site computation is the one
+// k_sweep_learned makes (features, network, head, stream-1 draws, proposal, energies, Hastings test), so the two
+// kernels take the same decisions. Waits are bounded: a plane that does not arrive sets bit 1 of the error word, a
+// tensor-core stage bit 0; either way the CTA drains its copies, frees its tensor memory and returns.
+struct LearnedPassArgs {
+  const CUtensorMap *tmaps;
+  float *dir;  // the buffer read and written (in place)
+  const RepDesc *reps;
+  RepState *st;
+  const FusedItem *items;
+  double *partials;  // [item][kPartials]: colour 0 writes, colour 1 adds
+  const unsigned long long *sweep_ctr;
+  const MlpTC *mlp_tc;
+  unsigned *err;
+  float kappa_max;
+  int cur, colour, measure;
+  long long timeout_ns;
+};
+
+constexpr int kLTY = 8, kLH = kLTY + 2, kLPF = RW * kLH, kLSlot = (3 * kLPF + 31) / 32 * 32, kLNS = 4;
+constexpr size_t kLearnedPassSmem = 128 + (size_t)kLNS * kLSlot * 4 + kLNS * 8 + sizeof(TcSmem) + 128;
+
+// Ghost copies of one updated site (half index j of the half-row row0 of parity h, component 0): along a periodic
+// y the site again at rows y + ny (y < 2) and y - ny (y >= ny - 2); along a periodic x, on each of those rows, half
+// index nx / 2 for half index 0 and half index -1 for nx / 2 - 1.
+static __device__ __noinline__ void learned_ghosts(float *row0, long long cs, int px, float vx, float vy, float vz,
+                                                   int j, int nx, int ny, int y, bool perx, bool pery) {
+  const float v[3] = {vx, vy, vz};
+  for (int iy = 0; iy < 3; iy++) {
+    if (iy == 1 && !(pery && y < 2)) continue;
+    if (iy == 2 && !(pery && y >= ny - 2)) continue;
+    float *rowp = row0 + (long long)(iy == 0 ? 0 : (iy == 1 ? ny : -ny)) * px;
+    if (iy > 0)
+      for (int q = 0; q < 3; q++) rowp[q * cs + j] = v[q];
+    if (perx && j == 0)
+      for (int q = 0; q < 3; q++) rowp[q * cs + (nx >> 1)] = v[q];
+    if (perx && j == (nx >> 1) - 1)
+      for (int q = 0; q < 3; q++) rowp[q * cs - 1] = v[q];
+  }
+}
+
+template <int POT, int GEO>
+__global__ void __launch_bounds__(kThreads, 2) k_learned_pass(ModelDev m, LearnedPassArgs a) {
+  static_assert(kThreads == 32 * kLTY, "one warp per tile row, one site per thread");
+  extern __shared__ __align__(128) unsigned char lp_dyn[];
+  unsigned char *smem_raw = smem_align128(lp_dyn);
+  float *slots = reinterpret_cast<float *>(smem_raw);
+  unsigned long long *bars = reinterpret_cast<unsigned long long *>(smem_raw + (size_t)kLNS * kLSlot * 4);
+  TcSmem &T = *reinterpret_cast<TcSmem *>(tc_align128(smem_raw + (size_t)kLNS * kLSlot * 4 + kLNS * 8));
+  __shared__ int s_fail;
+  __shared__ double red[kThreads / 32][kPartials];
+  const FusedItem it = a.items[blockIdx.x];
+  const RepDesc R = a.reps[it.rep];
+  const RepState St = a.st[it.rep];
+  const int tid = threadIdx.x;
+  const CUtensorMap *map = a.tmaps + 2 * it.rep + a.cur;
+  const int nx = R.nx, ny = R.ny, nz = R.nz;
+  const bool perx = R.periodic[0], pery = R.periodic[1], perz = R.periodic[2];
+  const int x0 = it.x0, y0 = it.y0, z0 = it.z0, z1 = it.z1, j0 = x0 >> 1;
+  const int colour = a.colour;
+  const bool measure = a.measure != 0;
+  const unsigned long long sweep = *a.sweep_ctr;
+  constexpr unsigned box_bytes = 3u * kLPF * 4u;
+  if (tid == 0) {
+    s_fail = 0;
+    for (int q = 0; q < kLNS; q++) mbar_init(&bars[q], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(map) : "memory");
+  }
+  tc_setup(T, a.mlp_tc);  // ends with a CTA barrier: the plane barriers are initialised for every thread
+  unsigned phase = 0;
+
+  const int pbeg = z0 - 1, pend = z1;
+  auto plane_exists = [&](int p) { return perz || (p >= 0 && p < nz); };
+  auto wrapz = [&](int p) { return p < 0 ? p + nz : (p >= nz ? p - nz : p); };
+  auto slot_ptr = [&](int p) -> float * { return slots + (size_t)((unsigned)(p - pbeg) % kLNS) * kLSlot; };
+  int last_issued = pbeg - 1;
+  auto issue = [&](int p) {  // thread 0 only
+    if (p > pend) return;
+    const int lp = p - pbeg;
+    last_issued = p;
+    unsigned long long *bar = &bars[(unsigned)lp % kLNS];
+    if (!plane_exists(p)) {
+      mbar_arrive(bar);
+      return;
+    }
+    mbar_expect_tx(bar, box_bytes);
+    tma_load_plane(slot_ptr(p), map, j0, y0 - 1 + GY, wrapz(p), bar);
+  };
+  int waited = pbeg - 1;
+  auto wait_plane = [&](int p) -> bool {
+    if (p <= pend && p > waited) {
+      const int lp = p - pbeg;
+      if (plane_exists(p) && !mbar_wait_bounded(&bars[(unsigned)lp % kLNS], ((unsigned)lp / kLNS) & 1u, a.timeout_ns))
+        s_fail = 1;
+    }
+    __syncthreads();
+    if (s_fail) return false;
+    if (p > waited) waited = p;
+    return true;
+  };
+  if (tid == 0)
+    for (int p = pbeg; p <= pbeg + 3; p++) issue(p);
+
+  const int r = tid >> 5, s = tid & 31;  // row y0 + r, half-row cell j0 + s
+  const int y = y0 + r, jb = 4 + s, j = j0 + s;
+  const bool live_row = y < ny;
+  const long long cs = R.comp;
+  unsigned accepted = 0;
+  double dacc[kPartials];
+#pragma unroll
+  for (int q = 0; q < kPartials; q++) dacc[q] = 0.0;
+  bool ok = wait_plane(z0 - 1) && wait_plane(z0);
+  bool tc_ok = true;
+  Vec3 pd{0.f, 0.f, 0.f};  // -z neighbour: plane k - 1, cell jb, this step's parity
+  if (ok && plane_exists(z0 - 1)) {
+    const float *q0 = slot_ptr(z0 - 1) + ((r + 1) * 2 + ((colour + y + z0) & 1)) * HALF + jb;
+    pd = Vec3{q0[0], q0[kLPF], q0[2 * kLPF]};
+  }
+  for (int k = z0; ok && k < z1; k++) {
+    ok = wait_plane(k + 1);
+    if (!ok) break;
+    if (tid == 0) issue(k + 3);
+    const int h = (colour + y + k) & 1;
+    const int x = 2 * j + h;
+    const bool valid = live_row && x < nx;
+    const float *cs_k = slot_ptr(k);
+    const float *above = plane_exists(k + 1) ? slot_ptr(k + 1) : nullptr;
+    const float *own = cs_k + ((r + 1) * 2 + h) * HALF + jb;
+    const float *oth = cs_k + ((r + 1) * 2 + (h ^ 1)) * HALF + jb - 1 + h;  // cells of x - 1, x + 1
+    auto ld3 = [&](const float *p) { return Vec3{p[0], p[kLPF], p[2 * kLPF]}; };
+    const Vec3 n = ld3(own);
+    const Vec3 xm = ld3(oth), xp = ld3(oth + 1);
+    Vec3 nb[6] = {xp, xm, ld3(own + RW), ld3(own - RW), above ? ld3(above + ((r + 1) * 2 + h) * HALF + jb)
+                                                              : Vec3{0.f, 0.f, 0.f}, pd};
+    float w[6];
+    w[0] = (perx || x + 1 < nx) ? 1.f : 0.f;
+    w[1] = (perx || x - 1 >= 0) ? 1.f : 0.f;
+    w[2] = (pery || y + 1 < ny) ? 1.f : 0.f;
+    w[3] = (pery || y - 1 >= 0) ? 1.f : 0.f;
+    w[4] = above ? 1.f : 0.f;
+    w[5] = plane_exists(k - 1) ? 1.f : 0.f;
+#pragma unroll
+    for (int d = 0; d < 6; d++)  // an absent neighbour is the zero vector, as the gathering kernel has it
+      if (w[d] == 0.f) nb[d] = Vec3{0.f, 0.f, 0.f};
+    pd = h ? xm : xp;  // the other-parity cell jb of plane k: the next step's -z neighbour
+    float f[kIn] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (valid) site_features(nb, w, St.T, f);
+    float o[kOut];
+    if (!cta_mlp_tc(T, phase, a.timeout_ns, f, o)) {  // CTA-uniform
+      tc_ok = false;
+      break;
+    }
+    if (!valid) continue;
+    int sid = -1;
+    float sz = 0.f;
+    if (GEO == GEO_SLAB) sid = slab_surface(k, nz, sz);
+    const Vec3 sn{0.f, 0.f, sz};
+    const Head hd = mlp_head(o, a.kappa_max);
+    const U4 u = site_draws(R.seed, sweep, (uint32_t)site_linear(R, x, y, k), 1);
+    const float em1 = expm1f(-2.f * hd.kappa);
+    const Vec3 nn = sample_proposal(hd, em1, u24(u.x), u24(u.y), u24(u.z), (u.x & 1u) != 0u);
+    float b_old, b_new;
+    bond_sum2<POT, false, true, float>(m, n, nn, nb, w, b_old, b_new);
+    const float s_old = single_energy<true>(m, n, sid, sn, St.elecE);
+    const float s_new = single_energy<true>(m, nn, sid, sn, St.elecE);
+    const float dE = __fadd_rn(__fadd_rn(b_new, s_new), -__fadd_rn(b_old, s_old));
+    bool acc;
+    if (St.T > 0.f) {  // u < e^{-dE/T} q(n) / q(n'), without logarithms
+      const float inv_den = -1.f / em1, e2k = 1.f + em1;
+      const float q_old = q4pi(dot(hd.mu, n), hd.kappa, inv_den, e2k), q_new = q4pi(dot(hd.mu, nn), hd.kappa, inv_den, e2k);
+      acc = u24(u.w) * q_new < __expf(-dE / St.T) * q_old;
+    } else {
+      acc = dE <= 0.f;
+    }
+    if (acc) {
+      float *row0 = a.dir + R.off + ((long long)k * R.py + (y + GY)) * R.px + h * R.hp + GH;
+      row0[j] = nn.x;
+      row0[cs + j] = nn.y;
+      row0[2 * cs + j] = nn.z;
+      if ((perx && (j == 0 || j == (nx >> 1) - 1)) || (pery && (y < 2 || y >= ny - 2)))
+        learned_ghosts(row0, cs, R.px, nn.x, nn.y, nn.z, j, nx, ny, y, perx, pery);
+      accepted++;
+    }
+    if (measure) {  // the site is final: colour 0 adds its single-site terms, colour 1 2 bond + single
+      const Vec3 nf = acc ? nn : n;
+      const float bf = acc ? b_new : b_old, sf = acc ? s_new : s_old;
+      dacc[0] += (double)(colour == 0 ? sf : __fadd_rn(__fmul_rn(2.f, bf), sf));
+      dacc[1] += (double)fmaf(1.5f * nf.x, nf.x, -0.5f);
+      dacc[2] += (double)(1.5f * nf.x * nf.y);
+      dacc[3] += (double)(1.5f * nf.x * nf.z);
+      dacc[4] += (double)fmaf(1.5f * nf.y, nf.y, -0.5f);
+      dacc[5] += (double)(1.5f * nf.y * nf.z);
+      dacc[6] += (double)fmaf(1.5f * nf.z, nf.z, -0.5f);
+      dacc[7] += (double)nf.x;
+      dacc[8] += (double)nf.y;
+      dacc[9] += (double)nf.z;
+    }
+  }
+  if (!ok || !tc_ok) {
+    if (tid == 0) {
+      atomicOr(a.err, ok ? 1u : 2u);
+      for (int q = max(waited + 1, last_issued - kLNS + 1); q <= last_issued; q++) {
+        if (!plane_exists(q)) continue;
+        const int lp = q - pbeg;
+        mbar_wait_bounded(&bars[(unsigned)lp % kLNS], ((unsigned)lp / kLNS) & 1u, a.timeout_ns);
+      }
+    }
+    tc_teardown(T);
+    return;
+  }
+  const unsigned wsum = __reduce_add_sync(0xffffffffu, accepted);
+  if ((tid & 31) == 0 && wsum) atomicAdd(&a.st[it.rep].acc, (unsigned long long)wsum);
+  if (measure) {
+    const int lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+    for (int q = 0; q < kPartials; q++) {
+      double v = dacc[q];
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+      if (lane == 0) red[warp][q] = v;
+    }
+    __syncthreads();
+    if (tid < kPartials) {
+      double v = 0.0;
+      for (int w2 = 0; w2 < kThreads / 32; w2++) v += red[w2][tid];
+      double *dst = a.partials + (long long)blockIdx.x * kPartials + tid;
+      *dst = colour == 0 ? v : *dst + v;
+    }
+  }
+  tc_teardown(T);
+}
+
+template <int POT>
+static cudaError_t learned_pass_pot(const ModelDev &m, const LearnedPassArgs &a, int geo, int n_items,
+                                    cudaStream_t stream) {
+  auto k = geo == GEO_SLAB ? k_learned_pass<POT, GEO_SLAB> : k_learned_pass<POT, GEO_BULK>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLearnedPassSmem);
+  if (e != cudaSuccess) return e;
+  k<<<n_items, kThreads, kLearnedPassSmem, stream>>>(m, a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_learned_pass(const LaunchCtx &c, int geo, const LearnedPassView &v, const LearnedMlp &mlp,
+                                float kappa_max, int measure, float *dir, int cur) {
+  if (v.n_items == 0) return cudaSuccess;
+  for (int colour = 0; colour < 2; colour++) {
+    LearnedPassArgs a;
+    a.tmaps = v.tmaps;
+    a.dir = dir;
+    a.reps = c.reps;
+    a.st = c.state;
+    a.items = v.items;
+    a.partials = v.partials;
+    a.sweep_ctr = c.sweep_ctr;
+    a.mlp_tc = mlp.tc;
+    a.err = mlp.err;
+    a.kappa_max = kappa_max;
+    a.cur = cur;
+    a.colour = colour;
+    a.measure = measure;
+    a.timeout_ns = 2000000000ll;
+    cudaError_t e;
+    if (c.model.potential == POT_GHRL)
+      e = learned_pass_pot<POT_GHRL>(c.model, a, geo, v.n_items, c.stream);
+    else if (c.model.potential == POT_PEAR)
+      e = learned_pass_pot<POT_PEAR>(c.model, a, geo, v.n_items, c.stream);
+    else
+      e = learned_pass_pot<POT_LL>(c.model, a, geo, v.n_items, c.stream);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 // ---- launchers -------------------------------------------------------------------------------------------------
 template <int POT, int GEO, bool TC>
 static void sweep_learned_one(const LaunchCtx &c, const BlockTable &t, int colour, const LearnedMlp &mlp,
@@ -891,7 +1171,8 @@ int learned_check_error(mcl_engine *e) {
   CKL(cudaStreamSynchronize(e->stream));
   if (v) {
     CKL(cudaMemsetAsync(e->d_lerr, 0, sizeof v, e->stream));
-    return fail(MCL_ERR_CUDA, "learned sweep: a tensor-core completion did not arrive within 2 s");
+    return fail(MCL_ERR_CUDA, (v & 2u) ? "learned sweep: a plane copy did not arrive within 2 s"
+                                       : "learned sweep: a tensor-core completion did not arrive within 2 s");
   }
   return MCL_OK;
 }
@@ -927,6 +1208,10 @@ int mcl_set_proposal(mcl_engine *e, const mcl_mlp *mlp, float kappa_max) {
   // tcgen05 unless MCL_LEARNED_MLP=mma selects the mma.sync warps (same network, same rounding points)
   const char *path = getenv("MCL_LEARNED_MLP");
   e->mlp_tc = !(path && strcmp(path, "mma") == 0);
+  // colour passes on streamed planes where the engine tiles (bulk, slab), unless MCL_LEARNED_KERNEL=gather
+  // selects the kernel that gathers each site's neighbours from global memory (same decisions)
+  const char *kern = getenv("MCL_LEARNED_KERNEL");
+  e->learned_pass = !(kern && strcmp(kern, "gather") == 0);
   return MCL_OK;
 }
 

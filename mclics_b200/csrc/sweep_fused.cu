@@ -20,6 +20,9 @@ static const FusedCfg kCfgs[kNumCfgs] = {{14, 256, 1, 0, 64}, {28, 512, 1, 0, 64
 
 struct FusedPlan {
   int cfg = 0, tx = 64, ty = 14, seg = 32;
+  FusedCfg C{};              // the tile configuration (kCfgs[cfg], or the learned plan's own)
+  bool learned = false;      // the learned colour passes' plan: its kernel sets its own shared-memory limit
+  FusedPlan *lplan = nullptr;  // that plan, built at the first learned sweep
   int seg_override = 0;  // planes per z segment chosen by the autotuner (0: heuristic)
   int n_items = 0;
   FusedItem *d_items = nullptr;
@@ -78,7 +81,7 @@ static int encode_map(CUtensorMap *map, float *base, const RepDesc &D, int cells
 // a multiple of the resident CTAs, with segments long enough that the extra planes of each stay cheap (fused: four
 // loaded, two of them computed; colour pass: two loaded).
 static void choose_segments(const mcl_engine *e, FusedPlan &P, int sms) {
-  const FusedCfg &C = kCfgs[P.cfg];
+  const FusedCfg &C = P.C;
   P.tx = C.tx;
   P.ty = C.ty;
   long long tiles = 0, maxz = 1;
@@ -118,14 +121,14 @@ static int choose_cfg(const mcl_engine *e) {
 static int prepare_kernel(mcl_engine *e, FusedPlan *P);
 
 static int build_items(mcl_engine *e, FusedPlan *P) {
+  if (!P->learned) P->C = kCfgs[P->cfg];
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device);
   choose_segments(e, *P, sms);
   std::vector<CUtensorMap> maps(2 * e->n_rep);
   for (int r = 0; r < e->n_rep; r++)
     for (int b = 0; b < 2; b++) {
-      int rc = encode_map(&maps[2 * r + b], e->d_dir[b], e->desc[r], P->tx / 2 + 8,
-                          P->ty + (kCfgs[P->cfg].kind ? 2 : 4));
+      int rc = encode_map(&maps[2 * r + b], e->d_dir[b], e->desc[r], P->tx / 2 + 8, P->ty + (P->C.kind ? 2 : 4));
       if (rc) return rc;
     }
   cudaFree(P->d_tmaps);
@@ -151,11 +154,11 @@ static int build_items(mcl_engine *e, FusedPlan *P) {
   CKF(cudaMalloc(&P->d_first, first.size() * sizeof(int)));
   CKF(cudaMemcpy(P->d_first, first.data(), first.size() * sizeof(int), cudaMemcpyHostToDevice));
   CKF(cudaMalloc(&P->d_partials, (size_t)P->n_items * kPartials * sizeof(double)));
-  const bool pass = kCfgs[P->cfg].kind == 1;
+  const bool pass = P->C.kind == 1;
   const int nsl = pass ? NSLP : NSL;
   const size_t slot_floats = ((size_t)3 * (P->tx + 16) * (P->ty + (pass ? 2 : 4)) + 31) / 32 * 32;
   P->smem = 128 + (size_t)nsl * slot_floats * sizeof(float) + nsl * sizeof(unsigned long long);
-  return prepare_kernel(e, P);
+  return P->learned ? MCL_OK : prepare_kernel(e, P);
 }
 
 int fused_create(mcl_engine *e) {
@@ -219,9 +222,44 @@ int fused_get_cfg(const mcl_engine *e, int *cfg, int *ty, int *seg, int *items) 
   return MCL_OK;
 }
 
+static void free_plan(FusedPlan *P) {
+  cudaFree(P->d_items);
+  cudaFree(P->d_tmaps);
+  cudaFree(P->d_partials);
+  cudaFree(P->d_first);
+}
+
+int fused_learned_view(mcl_engine *e, LearnedPassView *v) {
+  FusedPlan *P = e->fused;
+  if (!P) return fail(MCL_ERR_STATE, "the learned colour passes need the tiled sweep");
+  if (!P->lplan) {
+    FusedPlan *L = new FusedPlan();
+    L->learned = true;
+    L->C = FusedCfg{8, 256, 2, 1, 64};  // 64 x 8 tiles: 256 sites of a colour per plane, one tcgen05 batch
+    L->cfg = -1;
+    const int rc = build_items(e, L);
+    if (rc) {
+      free_plan(L);
+      delete L;
+      return rc;
+    }
+    P->lplan = L;
+  }
+  v->tmaps = P->lplan->d_tmaps;
+  v->items = P->lplan->d_items;
+  v->n_items = P->lplan->n_items;
+  v->partials = P->lplan->d_partials;
+  v->first = P->lplan->d_first;
+  return MCL_OK;
+}
+
 void fused_destroy(mcl_engine *e) {
   FusedPlan *P = e->fused;
   if (!P) return;
+  if (P->lplan) {
+    free_plan(P->lplan);
+    delete P->lplan;
+  }
   cudaFree(P->d_items);
   cudaFree(P->d_tmaps);
   cudaFree(P->d_partials);

@@ -195,3 +195,51 @@ def test_learned_sweep_keeps_the_equilibrium(trained):
         assert abs(a.mean() - b.mean()) < 4 * se + 1e-4, (a.mean(), b.mean(), se)
     plain.close()
     learned.close()
+
+
+LEARNED_SHAPES = [
+    # (potential, nx, ny, nz, geometry, periodic)
+    ("ll", 64, 16, 20, "bulk", (1, 1, 1)),
+    ("ll", 72, 22, 30, "bulk", (1, 1, 1)),    # ragged x and y tiles, several z segments
+    ("ll", 30, 18, 26, "bulk", (0, 0, 0)),    # free everywhere
+    ("ll", 2, 2, 2, "bulk", (1, 1, 1)),       # ghosts of ghosts
+    ("ll", 6, 4, 4, "bulk", (1, 0, 1)),
+    ("ghrl", 68, 20, 17, "slab", (1, 1, 0)),  # anchoring on both plates
+    ("pear", 40, 12, 9, "slab", (0, 1, 0)),
+]
+
+
+@pytest.mark.parametrize("shape", LEARNED_SHAPES, ids=["%s-%dx%dx%d-%s-%s" % (s[0], s[1], s[2], s[3], s[4],
+                                                                             "".join(map(str, s[5])))
+                                                       for s in LEARNED_SHAPES])
+def test_learned_passes_match_the_gathering_kernel(shape, monkeypatch):
+    """The learned colour passes (planes in shared memory, one tcgen05 batch per plane) and the kernel that gathers
+    each site's neighbours from global memory make every per-site computation alike, so they take the same
+    decisions: identical directors and acceptance, observables equal up to the order of the sums."""
+    pot, nx, ny, nz, geo, per = shape
+    surf = {"slab": [("homeotropic", 1.2, 0, 0), ("fg", 0.6, 0, 0)]}.get(geo, [])
+    if pot == "ghrl":
+        model = M.Model("ghrl", k=(1.0, 0.5, 1.5), surfaces=surf)
+    elif pot == "pear":
+        model = M.Model("pear", A=1.5, B1=0.09, C=0.3, surfaces=surf)
+    else:
+        model = M.Model("ll", surfaces=surf)
+    params = perturbed_params(4)
+    out = {}
+    for kern in ("gather", "pass"):
+        if kern == "gather":
+            monkeypatch.setenv("MCL_LEARNED_KERNEL", "gather")
+        else:
+            monkeypatch.delenv("MCL_LEARNED_KERNEL", raising=False)
+        e = M.Engine(model, [M.Replica(nx, ny, nz, geo, per, T=0.9, seed=21)], M.SCHED_CHECKER2)
+        e.upload(0, rand_dirs(nx * ny * nz, 8))
+        e.set_sweep_counter(17)
+        e.set_proposal(params)
+        e.sweeps(3, measure=True)
+        out[kern] = (e.download(0), e.series(0))
+        e.close()
+    (a, sa), (b, sb) = out["gather"], out["pass"]
+    np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(sa["acceptance"], sb["acceptance"])
+    np.testing.assert_allclose(sa["energy"], sb["energy"], rtol=2e-6, atol=2e-6)
+    np.testing.assert_allclose(sa["q"], sb["q"], rtol=0, atol=2e-7)
