@@ -200,6 +200,7 @@ void fused_plan_candidates(const mcl_engine *e, std::vector<std::pair<int, int>>
   for (int cfg = 0; cfg < kNumCfgs; cfg++) {
     FusedPlan P;
     P.cfg = cfg;
+    P.C = kCfgs[cfg];
     choose_segments(e, P, sms);
     std::vector<int> segs = {P.seg, P.seg * 2, (P.seg + 1) / 2, maxz};
     std::sort(segs.begin(), segs.end());
