@@ -12,10 +12,11 @@ reference's thermalGPU loop. Metric: site updates per second (whole job, all GPU
              lattice (211 MB padded) is larger than L2 (126 MB), so no flush is needed between steps. The tile
              plan is chosen by mcl_autotune before timing, and the K steps are one mcl_sweeps call replaying a
              captured CUDA graph of the sweeps.
-  e2e        the same steps through the C ABI, one call sequence per step as a drop-in caller makes it, host
+  e2e        the same steps through the C ABI, one mcl_sweeps_io call per step as a drop-in caller makes it, host
              buffers and host<->device copies inside the timed region: the step's input (the temperature of every
-             replica) goes up from pinned host memory, the sweep runs, and the step's result (the observables
-             record of every replica) comes down to the host.
+             replica) goes up through the engine's pinned staging, the sweep runs, and the step's result (the
+             observables record of every replica, with the sweep kernel's error word) comes down to the host; one
+             host synchronisation per step.
   e2e_reference_data_movement  the same, plus the whole director field down every step, as the reference's GPU
              loop moves it (it computes Q on the host after every measurement sweep, src/evolve_thermal.cu:90;
              this engine computes it on the device, so a caller needs the field only for snapshots).
@@ -316,7 +317,8 @@ def gpu_arm(args, rank, world, local_rank):
     # end to end through the C ABI with host buffers, all replicas: temperatures up, the step's observables down
     # (and, second, also the whole director field down every step, the reference GPU loop's data movement)
     host_ni = [torch.empty(3 * n, dtype=torch.float32, pin_memory=True) for n in sizes]
-    host_T = torch.tensor([r["T"] for r in reps], dtype=torch.float32, pin_memory=True)
+    host_T = np.array([r["T"] for r in reps], dtype=np.float32)
+    host_obs = np.zeros(len(reps), M.OBS_DTYPE)
 
     def e2e_loop(lattice_down):
         torch.cuda.synchronize()
@@ -324,12 +326,9 @@ def gpu_arm(args, rank, world, local_rank):
             torch.distributed.barrier()
         t0 = time.perf_counter()
         for _ in range(args.steps):
-            for i in range(len(reps)):
-                eng.set_temperature(float(host_T[i]), i)
-            eng.sweeps(1, measure=True)
-            for i in range(len(reps)):
-                eng.series(i, eng.series_length() - 1, 1)
-                if lattice_down:
+            eng.sweeps_io(1, host_T, host_obs)  # temperatures up, one measured sweep, its records down
+            if lattice_down:
+                for i in range(len(reps)):
                     M.check(M.lib().mcl_download_directors(eng._h, i, host_ni[i].data_ptr()))
         return time.perf_counter() - t0
 
@@ -617,10 +616,10 @@ def main():
         "scaling": "strong" if sharded else "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config,
         "e2e": {"value": e2e, "unit": "site-updates/s", "h2d_bytes_per_step": 4 * res["n_rep"],
-                "d2h_bytes_per_step": 144 * res["n_rep"]},
+                "d2h_bytes_per_step": 144 * res["n_rep"] + 4},
         "e2e_reference_data_movement": {"value": e2e_lat, "unit": "site-updates/s",
                                         "h2d_bytes_per_step": 4 * res["n_rep"],
-                                        "d2h_bytes_per_step": 144 * res["n_rep"] + 12 * res["sites"],
+                                        "d2h_bytes_per_step": 144 * res["n_rep"] + 4 + 12 * res["sites"],
                                         "note": "plus the whole director field down every step, as the "
                                                 "reference's GPU loop copies it for its host-side Q tensor"},
         "gpu_launches": res["launches"],

@@ -126,6 +126,12 @@ int mcl_get_sweep_counter(mcl_engine *e, unsigned long long *sweep);
  * to the engine's series (energy_calculator_GPU + Q_tensor + eigen, done on the device). Asynchronous: returns
  * after enqueueing; errors of the device work surface at the next synchronising call. */
 int mcl_sweeps(mcl_engine *e, int n, int measure);
+/* One step of a caller's measurement loop in one call and one host synchronisation: T (n_replicas floats, or
+ * null to keep the temperatures) goes up through pinned staging, n measured sweeps run as mcl_sweeps(e, n, 1),
+ * and their records come down into out[s * n_replicas + r] (sweep s, replica r), together with the kernels'
+ * error words. The same as mcl_set_temperature per replica, mcl_sweeps and mcl_read_series (the loop of
+ * src/evolve_thermal.cu:78-106), without their separate round trips. */
+int mcl_sweeps_io(mcl_engine *e, int n, const float *T, mcl_observables *out);
 /* Number of records in the series; reading copies them to the host (synchronises). */
 int mcl_series_length(mcl_engine *e, int *n);
 int mcl_read_series(mcl_engine *e, int replica, int first, int count, mcl_observables *out);
@@ -230,9 +236,10 @@ int mcl_zslab_pack(mcl_engine *e, float *send_lo, float *send_hi);          /* n
 int mcl_zslab_unpack(mcl_engine *e, const float *recv_lo, const float *recv_hi); /* null: no neighbour there */
 int mcl_zslab_sums(mcl_engine *e, int measure, double *d_sums);
 int mcl_zslab_finalize(mcl_engine *e, const double *d_sums, int measure);
-/* With enable != 0, mcl_sweeps replays a captured CUDA graph of two fused sweeps (captured at the first call, again
- * after the plan, the series buffer or the test hooks change) instead of launching kernels one by one; results are
- * identical. Profiling (mcl_profile) uses direct launches. */
+/* With enable != 0, mcl_sweeps (and mcl_sweeps_io) replay a captured CUDA graph of one sweep (colour-pass plans)
+ * or two (the ping-pong fused plans 0 and 1), captured at the first call and again after the plan, the series buffer
+ * or the test hooks change, instead of launching kernels one by one; results are identical. Profiling (mcl_profile)
+ * uses direct launches. */
 int mcl_set_graphs(mcl_engine *e, int enable);
 
 /* ---- Learned Metropolis-Hastings proposal (no counterpart in the reference) ----------------------------------

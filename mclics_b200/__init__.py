@@ -86,6 +86,7 @@ def lib():
             "mcl_set_sweep_counter": [vp, ctypes.c_ulonglong],
             "mcl_get_sweep_counter": [vp, P(ctypes.c_ulonglong)],
             "mcl_sweeps": [vp, i, i],
+            "mcl_sweeps_io": [vp, i, vp, vp],
             "mcl_series_length": [vp, P(i)],
             "mcl_read_series": [vp, i, i, i, vp],
             "mcl_clear_series": [vp],
@@ -276,6 +277,24 @@ class Engine:
 
     def sweeps(self, n, measure=False):
         check(lib().mcl_sweeps(self._h, n, 1 if measure else 0))
+
+    def sweeps_io(self, n, T=None, out=None):
+        """n measured sweeps in one call: T (one float32 per replica, or None to keep the temperatures) goes up, the
+        n x replicas observables records come back (in `out` when given, an OBS_DTYPE array of that size)."""
+        n_rep = self.n
+        if out is None:
+            out = np.zeros(n * n_rep, OBS_DTYPE)
+        elif out.dtype != OBS_DTYPE or out.size < n * n_rep or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a contiguous OBS_DTYPE array of at least {n * n_rep} records")
+        tp = None
+        if T is not None:
+            if not (isinstance(T, np.ndarray) and T.dtype == np.float32 and T.flags.c_contiguous):
+                T = np.ascontiguousarray(T, dtype=np.float32)
+            if T.size != n_rep:
+                raise ValueError(f"T needs {n_rep} values, got {T.size}")
+            tp = T.ctypes.data
+        check(lib().mcl_sweeps_io(self._h, n, tp, out.ctypes.data))
+        return out
 
     def series_length(self):
         v = ctypes.c_int()

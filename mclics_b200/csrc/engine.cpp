@@ -135,9 +135,13 @@ static void drop_graphs(mcl_engine *e) {
   e->graph_series = nullptr;
 }
 
-// Captures two fused sweeps (one per ping-pong parity, starting from buffer e->cur) as a graph. Every per-sweep
-// quantity the kernels use (sweep counter, temperatures, ang_var, series length) lives in device memory, so a
-// replay does exactly what two direct calls would.
+// Sweeps per captured graph: one for the in-place colour passes, two for the ping-pong fused kernel (one per
+// buffer parity, so that a replay leaves the buffers where it found them).
+static int graph_sweeps(const mcl_engine *e) { return fused_is_pass_plan(e) ? 1 : 2; }
+
+// Captures graph_sweeps(e) sweeps starting from buffer e->cur as a graph. Every per-sweep quantity the kernels use
+// (sweep counter, temperatures, ang_var, series length) lives in device memory, so a replay does exactly what the
+// same direct calls would.
 static int capture_graph(mcl_engine *e, int m) {
   if (e->graph[m]) cudaGraphExecDestroy(e->graph[m]);
   e->graph[m] = nullptr;
@@ -145,8 +149,8 @@ static int capture_graph(mcl_engine *e, int m) {
   CK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
   const int cur0 = e->cur;
   const long long l0 = e->launches;
-  int rc = fused_sweep(e, m != 0, nullptr, nullptr);
-  if (!rc) rc = fused_sweep(e, m != 0, nullptr, nullptr);
+  int rc = MCL_OK;
+  for (int s = 0; s < graph_sweeps(e) && !rc; s++) rc = fused_sweep(e, m != 0, nullptr, nullptr);
   const cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
   e->cur = cur0;
   e->launches = l0;
@@ -421,6 +425,7 @@ int mcl_destroy(mcl_engine *e) {
   cudaFree(e->d_probe_len);
   cudaFree(e->d_partials);
   cudaFree(e->d_dec);
+  cudaFreeHost(e->h_io);
   for (cudaEvent_t ev : e->ev_pool) cudaEventDestroy(ev);
   if (e->own_stream) cudaStreamDestroy(e->own_stream);
   delete e;
@@ -551,7 +556,8 @@ int mcl_sweeps(mcl_engine *e, int n, int measure) {
   if (measure && (rc = ensure_series(e, e->series_len + n))) return rc;
   const bool use_fused = e->fused && !e->record_dec && !e->d_mlp;
   if (use_fused && (rc = refresh_ghosts(e))) return rc;
-  if (use_fused && e->use_graphs && !e->profile && n >= 2) {
+  const int per_graph = use_fused ? graph_sweeps(e) : 2;
+  if (use_fused && e->use_graphs && !e->profile && n >= per_graph) {
     const int m = measure ? 1 : 0;
     if (!e->graph[m] || (m && e->graph_series != (const void *)e->d_series)) {
       if ((rc = capture_graph(e, m))) return rc;
@@ -561,10 +567,10 @@ int mcl_sweeps(mcl_engine *e, int n, int measure) {
       if (measure) e->series_len++;
       n--;
     }
-    for (; n >= 2; n -= 2) {
+    for (; n >= per_graph; n -= per_graph) {
       CK(cudaGraphLaunch(e->graph[m], e->stream));
-      e->launches += 2 * fused_launches_per_sweep(e);
-      if (measure) e->series_len += 2;
+      e->launches += per_graph * fused_launches_per_sweep(e);
+      if (measure) e->series_len += per_graph;
     }
   }
   for (int s = 0; s < n; s++) {
@@ -627,6 +633,54 @@ int mcl_sweeps(mcl_engine *e, int n, int measure) {
     }
     if (measure) e->series_len++;
   }
+  return MCL_OK;
+}
+
+static void to_public(const ObsRecord &o, mcl_observables *p);
+
+int mcl_sweeps_io(mcl_engine *e, int n, const float *T, mcl_observables *out) {
+  if (!e) return fail(MCL_ERR_ARG, "null engine");
+  if (n < 1) return fail(MCL_ERR_ARG, "mcl_sweeps_io: n must be >= 1 (got %d)", n);
+  if (!out) return fail(MCL_ERR_ARG, "null output");
+  if (e->zslab) return fail(MCL_ERR_STATE, "mcl_sweeps_io: a z-slab engine sweeps through the mcl_zslab_* calls");
+  if (T)
+    for (int r = 0; r < e->n_rep; r++)
+      if (!(T[r] >= 0.f) || !isfinite(T[r]))
+        return fail(MCL_ERR_ARG, "temperature of replica %d must be finite and >= 0 (got %g)", r, T[r]);
+  // pinned staging: two error words, the temperatures, the records (64-byte aligned parts)
+  const size_t t_off = 64, rec_off = t_off + ((size_t)e->n_rep * sizeof(float) + 63) / 64 * 64;
+  const size_t rec_bytes = (size_t)n * e->n_rep * sizeof(ObsRecord), need = rec_off + rec_bytes;
+  if (e->io_inflight || need > e->h_io_bytes) CK(cudaStreamSynchronize(e->stream));
+  e->io_inflight = false;
+  if (need > e->h_io_bytes) {
+    cudaFreeHost(e->h_io);
+    e->h_io = nullptr;
+    e->h_io_bytes = 0;
+    CK(cudaHostAlloc(&e->h_io, need, cudaHostAllocDefault));
+    e->h_io_bytes = need;
+  }
+  unsigned *words = (unsigned *)e->h_io;
+  float *hT = (float *)((char *)e->h_io + t_off);
+  ObsRecord *rec = (ObsRecord *)((char *)e->h_io + rec_off);
+  words[0] = words[1] = 0;
+  if (T) {
+    memcpy(hT, T, (size_t)e->n_rep * sizeof(float));
+    e->io_inflight = true;
+    CK(cudaMemcpy2DAsync((char *)e->d_state + offsetof(RepState, T), sizeof(RepState), hT, sizeof(float),
+                         sizeof(float), e->n_rep, cudaMemcpyHostToDevice, e->stream));
+  }
+  const int first = e->series_len;
+  int rc = mcl_sweeps(e, n, 1);
+  if (rc) return rc;
+  e->io_inflight = true;
+  CK(cudaMemcpyAsync(rec, e->d_series + (size_t)first * e->n_rep, rec_bytes, cudaMemcpyDeviceToHost, e->stream));
+  if (unsigned *w = fused_error_word(e)) CK(cudaMemcpyAsync(&words[0], w, sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream));
+  if (e->d_lerr) CK(cudaMemcpyAsync(&words[1], e->d_lerr, sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  e->io_inflight = false;
+  if ((rc = fused_report_error(e, words[0]))) return rc;
+  if ((rc = learned_report_error(e, words[1]))) return rc;
+  for (size_t i = 0; i < (size_t)n * e->n_rep; i++) to_public(rec[i], out + i);
   return MCL_OK;
 }
 

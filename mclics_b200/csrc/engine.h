@@ -19,6 +19,8 @@ struct FusedPlan;  // fused tiled sweep (sweep_fused.cu)
 struct MlpDev;     // learned proposal weights in device layout (learned.cu)
 struct MlpTC;      // the same in the tcgen05 layout (mlp_tc.cuh)
 int learned_check_error(mcl_engine *e);
+// A learned-sweep error word read by the caller: non-zero is cleared and turned into MCL_ERR_CUDA.
+int learned_report_error(mcl_engine *e, unsigned word);
 
 }  // namespace mcl
 
@@ -76,10 +78,13 @@ struct mcl_engine {
   double *d_xpart = nullptr;   // scratch of mcl_measure_extras (allocated at its first call)
   float kappa_max = 500.f;
   bool adapt = true;           // ang_var adaptation after each sweep (the reference's behaviour)
-  bool use_graphs = false;     // fused sweeps replayed from a captured CUDA graph of two sweeps
-  cudaGraphExec_t graph[2] = {nullptr, nullptr};  // [measure]: two fused sweeps starting from buffer graph_cur
+  bool use_graphs = false;     // fused sweeps replayed from captured CUDA graphs (one or two sweeps each)
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};  // [measure]: the sweeps of one replay, from buffer graph_cur
   int graph_cur[2] = {0, 0};
   const void *graph_series = nullptr;             // series buffer the measuring graph writes
+  void *h_io = nullptr;      // pinned staging of mcl_sweeps_io: error words, temperatures, observables records
+  size_t h_io_bytes = 0;
+  bool io_inflight = false;  // copies that read or write h_io may still be queued (an error return before the sync)
 
   mcl::LaunchCtx ctx() const {
     mcl::LaunchCtx c;

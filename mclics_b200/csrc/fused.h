@@ -18,6 +18,10 @@ int fused_sweep(mcl_engine *e, bool measure, cudaEvent_t ev0, cudaEvent_t ev1);
 namespace mcl {
 // Reads and clears the fused kernel's error word (synchronises); MCL_ERR_CUDA if a TMA wait timed out.
 int fused_check_error(mcl_engine *e);
+// The device address of that error word (null without the tiled sweep), and the report of a word read from it
+// elsewhere: a non-zero word is cleared and turned into MCL_ERR_CUDA.
+unsigned int *fused_error_word(mcl_engine *e);
+int fused_report_error(mcl_engine *e, unsigned int word);
 // Test hook: wait limit in ns (> 0 to change) and whether the first TMA load of every CTA is withheld.
 void fused_set_test_hooks(mcl_engine *e, long long timeout_ns, int skip_first_load);
 // Tile configuration: 0: fused, 64 x 14 tiles, 256 threads; 1: fused, 64 x 28, 512 threads; 2: colour passes,

@@ -1169,12 +1169,14 @@ int learned_check_error(mcl_engine *e) {
   unsigned v = 0;
   CKL(cudaMemcpyAsync(&v, e->d_lerr, sizeof v, cudaMemcpyDeviceToHost, e->stream));
   CKL(cudaStreamSynchronize(e->stream));
-  if (v) {
-    CKL(cudaMemsetAsync(e->d_lerr, 0, sizeof v, e->stream));
-    return fail(MCL_ERR_CUDA, (v & 2u) ? "learned sweep: a plane copy did not arrive within 2 s"
-                                       : "learned sweep: a tensor-core completion did not arrive within 2 s");
-  }
-  return MCL_OK;
+  return learned_report_error(e, v);
+}
+
+int learned_report_error(mcl_engine *e, unsigned v) {
+  if (!v || !e->d_lerr) return MCL_OK;
+  CKL(cudaMemsetAsync(e->d_lerr, 0, sizeof v, e->stream));
+  return fail(MCL_ERR_CUDA, (v & 2u) ? "learned sweep: a plane copy did not arrive within 2 s"
+                                     : "learned sweep: a tensor-core completion did not arrive within 2 s");
 }
 }  // namespace mcl
 

@@ -400,13 +400,17 @@ int fused_check_error(mcl_engine *e) {
   unsigned int v = 0;
   CKF(cudaMemcpyAsync(&v, e->fused->d_err, sizeof v, cudaMemcpyDeviceToHost, e->stream));
   CKF(cudaStreamSynchronize(e->stream));
-  if (v) {
-    unsigned int zero = 0;
-    CKF(cudaMemcpy(e->fused->d_err, &zero, sizeof zero, cudaMemcpyHostToDevice));
-    return fail(MCL_ERR_CUDA, "fused sweep: a TMA load did not complete within %.3f s (error word 0x%x)",
-                e->fused->timeout_ns * 1e-9, v);
-  }
-  return MCL_OK;
+  return fused_report_error(e, v);
+}
+
+unsigned int *fused_error_word(mcl_engine *e) { return e->fused ? e->fused->d_err : nullptr; }
+
+int fused_report_error(mcl_engine *e, unsigned int v) {
+  if (!v || !e->fused) return MCL_OK;
+  unsigned int zero = 0;
+  CKF(cudaMemcpy(e->fused->d_err, &zero, sizeof zero, cudaMemcpyHostToDevice));
+  return fail(MCL_ERR_CUDA, "fused sweep: a TMA load did not complete within %.3f s (error word 0x%x)",
+              e->fused->timeout_ns * 1e-9, v);
 }
 
 void fused_set_test_hooks(mcl_engine *e, long long timeout_ns, int skip_first_load) {
