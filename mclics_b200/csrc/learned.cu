@@ -308,6 +308,83 @@ __device__ __forceinline__ bool cta_mlp_tc(TcSmem &S, unsigned &phase, long long
   return true;
 }
 
+// ---- the same network per warpgroup: 128 threads evaluate their own 128-row tile, independently of the CTA's
+// other warpgroup (named barrier 1 + wg, their own commit mbarrier), so that one warpgroup's tensor-core round trips
+// overlap the other's scalar work.
+__device__ __forceinline__ void wg_bar(int wg) { asm volatile("bar.sync %0, 128;" ::"r"(1 + wg) : "memory"); }
+
+template <typename Issue>
+__device__ __forceinline__ bool wg_stage(unsigned long long *bar, volatile int *wfail, unsigned &phase,
+                                         long long timeout_ns, int wg, Issue issue) {
+  tc_fence_async_smem();
+  tc_fence_before();
+  wg_bar(wg);
+  if ((threadIdx.x & 127) == 0) {
+    tc_fence_after();
+    issue();
+    tc_commit(bar);
+  }
+  const bool ok = tc_wait(bar, phase, timeout_ns);
+  if (!ok) atomicOr((int *)wfail, 1);
+  wg_bar(wg);
+  if (*wfail) {  // wait (bounded) for the commit in flight before the tensor memory is freed
+    tc_wait(bar, phase, timeout_ns);
+    return false;
+  }
+  phase ^= 1u;
+  tc_fence_after();
+  return true;
+}
+
+// cta_mlp_tc for the warpgroup wg = threadIdx.x / 128 (tile wg, tensor-memory columns 64 wg .. 64 wg + 63); false
+// (warpgroup-uniform) after a tensor-core timeout.
+__device__ __forceinline__ bool wg_mlp_tc(TcSmem &S, unsigned long long *bar, volatile int *wfail, unsigned &phase,
+                                          long long timeout_ns, const float (&f)[kIn], float (&o)[kOut]) {
+  const int tid = threadIdx.x, wg = tid >> 7, row = tid & 127;
+  uint8_t *a1 = S.a1 + wg * kTcA1;
+  uint4 lo;
+  lo.x = pack2(f[0], f[1]);
+  lo.y = pack2(f[2], f[3]);
+  lo.z = pack2(f[4], f[5]);
+  lo.w = pack2(f[6], 0.f);
+  *reinterpret_cast<uint4 *>(a1 + core_off(row, 0, 16)) = lo;
+  *reinterpret_cast<uint4 *>(a1 + core_off(row, 8, 16)) = make_uint4(0u, 0u, 0u, 0u);
+  constexpr uint32_t id64 = tc_idesc(128, 64), id16 = tc_idesc(128, 16);
+  const uint32_t dcol = S.tmem + wg * 64;
+  if (!wg_stage(bar, wfail, phase, timeout_ns, wg,
+                [&] { tc_mma(dcol, tc_desc(a1, 128, 256), tc_desc(S.w1, 128, 256), id64, 0); }))
+    return false;
+  const uint32_t tcol = dcol + ((uint32_t)(32 * ((tid >> 5) & 3)) << 16);
+  uint8_t *a2 = S.a2 + wg * kTcA2;
+#pragma unroll
+  for (int hf = 0; hf < 2; hf++) {
+    float v[32];
+    tc_ld32(tcol + 32 * hf, v);
+    tc_act_store(a2, row, 32 * hf, v, S.b1);
+  }
+  if (!wg_stage(bar, wfail, phase, timeout_ns, wg, [&] {
+        for (int ks = 0; ks < 4; ks++)
+          tc_mma(dcol, tc_desc(a2 + ks * 256, 128, 1024), tc_desc(S.w2 + ks * 256, 128, 1024), id64, ks > 0);
+      }))
+    return false;
+#pragma unroll
+  for (int hf = 0; hf < 2; hf++) {  // layer 2 has completed: its input tile may be overwritten with h2
+    float v[32];
+    tc_ld32(tcol + 32 * hf, v);
+    tc_act_store(a2, row, 32 * hf, v, S.b2);
+  }
+  if (!wg_stage(bar, wfail, phase, timeout_ns, wg, [&] {
+        for (int ks = 0; ks < 4; ks++)
+          tc_mma(dcol, tc_desc(a2 + ks * 256, 128, 1024), tc_desc(S.w3 + ks * 256, 128, 1024), id16, ks > 0);
+      }))
+    return false;
+  float v4[4];
+  tc_ld4(tcol, v4);
+#pragma unroll
+  for (int k = 0; k < kOut; k++) o[k] = v4[k] + S.b3[k];
+  return true;
+}
+
 // Network outputs of feature rows on tcgen05 (the same outputs as k_mlp_forward).
 __global__ void __launch_bounds__(kTcRows) k_mlp_forward_tc(const MlpTC *__restrict__ w,
                                                             const float *__restrict__ feat, long long n,
@@ -832,7 +909,8 @@ struct LearnedPassArgs {
 };
 
 constexpr int kLTY = 8, kLH = kLTY + 2, kLPF = RW * kLH, kLSlot = (3 * kLPF + 31) / 32 * 32, kLNS = 4;
-constexpr size_t kLearnedPassSmem = 128 + (size_t)kLNS * kLSlot * 4 + kLNS * 8 + sizeof(TcSmem) + 128;
+// plane slots, their full and empty barriers, the tcgen05 operands
+constexpr size_t kLearnedPassSmem = 128 + (size_t)kLNS * kLSlot * 4 + 2 * kLNS * 8 + sizeof(TcSmem) + 128;
 
 // Ghost copies of one updated site (half index j of the half-row row0 of parity h, component 0): along a periodic
 // y the site again at rows y + ny (y < 2) and y - ny (y >= ny - 2); along a periodic x, on each of those rows, half
@@ -853,15 +931,22 @@ static __device__ __noinline__ void learned_ghosts(float *row0, long long cs, in
   }
 }
 
+// The two warpgroups (tile rows 0-3 and 4-7) run decoupled: each waits for the planes itself, evaluates its
+// 128-row tile on the tensor cores with its own barriers, and every warp releases a plane slot (empty barrier) once
+// it has loaded its neighbours from it; thread 0 refills a slot only after all eight warps released it. A warpgroup
+// may run up to a plane ahead of the other, so one's tensor-core round trips overlap the other's scalar work.
 template <int POT, int GEO>
 __global__ void __launch_bounds__(kThreads, 2) k_learned_pass(ModelDev m, LearnedPassArgs a) {
   static_assert(kThreads == 32 * kLTY, "one warp per tile row, one site per thread");
+  static_assert(kThreads == 2 * 128, "two warpgroups, one 128-row tile each");
   extern __shared__ __align__(128) unsigned char lp_dyn[];
   unsigned char *smem_raw = smem_align128(lp_dyn);
   float *slots = reinterpret_cast<float *>(smem_raw);
   unsigned long long *bars = reinterpret_cast<unsigned long long *>(smem_raw + (size_t)kLNS * kLSlot * 4);
-  TcSmem &T = *reinterpret_cast<TcSmem *>(tc_align128(smem_raw + (size_t)kLNS * kLSlot * 4 + kLNS * 8));
-  __shared__ int s_fail;
+  unsigned long long *ebars = bars + kLNS;  // slot released by all eight warps
+  TcSmem &T = *reinterpret_cast<TcSmem *>(tc_align128(smem_raw + (size_t)kLNS * kLSlot * 4 + 2 * kLNS * 8));
+  __shared__ unsigned long long s_mma[2];  // tensor-core commits, one barrier per warpgroup
+  __shared__ int s_wfail[2];               // per warpgroup: bit 0 a tensor-core wait, bit 1 a plane wait timed out
   __shared__ double red[kThreads / 32][kPartials];
   const FusedItem it = a.items[blockIdx.x];
   const RepDesc R = a.reps[it.rep];
@@ -876,12 +961,19 @@ __global__ void __launch_bounds__(kThreads, 2) k_learned_pass(ModelDev m, Learne
   const unsigned long long sweep = *a.sweep_ctr;
   constexpr unsigned box_bytes = 3u * kLPF * 4u;
   if (tid == 0) {
-    s_fail = 0;
-    for (int q = 0; q < kLNS; q++) mbar_init(&bars[q], 1);
+    s_wfail[0] = s_wfail[1] = 0;
+    for (int q = 0; q < kLNS; q++) {
+      mbar_init(&bars[q], 1);
+      mbar_init(&ebars[q], kThreads / 32);
+    }
+    mbar_init(&s_mma[0], 1);
+    mbar_init(&s_mma[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("prefetch.tensormap [%0];" ::"l"(map) : "memory");
   }
   tc_setup(T, a.mlp_tc);  // ends with a CTA barrier: the plane barriers are initialised for every thread
+  const int wg = tid >> 7, lane = tid & 31;
+  volatile int *wfail = &s_wfail[wg];
   unsigned phase = 0;
 
   const int pbeg = z0 - 1, pend = z1;
@@ -889,32 +981,43 @@ __global__ void __launch_bounds__(kThreads, 2) k_learned_pass(ModelDev m, Learne
   auto wrapz = [&](int p) { return p < 0 ? p + nz : (p >= nz ? p - nz : p); };
   auto slot_ptr = [&](int p) -> float * { return slots + (size_t)((unsigned)(p - pbeg) % kLNS) * kLSlot; };
   int last_issued = pbeg - 1;
-  auto issue = [&](int p) {  // thread 0 only
-    if (p > pend) return;
+  auto issue = [&](int p) -> bool {  // thread 0 only; false if the slot was not released in time
+    if (p > pend) return true;
     const int lp = p - pbeg;
+    const unsigned sl = (unsigned)lp % kLNS;
+    if (lp >= kLNS && !mbar_wait_bounded(&ebars[sl], ((unsigned)lp / kLNS - 1u) & 1u, a.timeout_ns)) return false;
     last_issued = p;
-    unsigned long long *bar = &bars[(unsigned)lp % kLNS];
+    unsigned long long *bar = &bars[sl];
     if (!plane_exists(p)) {
       mbar_arrive(bar);
-      return;
+      return true;
     }
     mbar_expect_tx(bar, box_bytes);
     tma_load_plane(slot_ptr(p), map, j0, y0 - 1 + GY, wrapz(p), bar);
+    return true;
+  };
+  auto release = [&](int p) {  // this warp has loaded what it needs from plane p
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&ebars[(unsigned)(p - pbeg) % kLNS]);
   };
   int waited = pbeg - 1;
-  auto wait_plane = [&](int p) -> bool {
+  bool pfail = false;  // thread 0: a slot was not released in time (published before its next plane barrier)
+  // Flags are written only before a warpgroup barrier that precedes their reads, so every thread of the warpgroup
+  // reads the same value.
+  auto wait_plane = [&](int p) -> bool {  // warpgroup-uniform result
     if (p <= pend && p > waited) {
       const int lp = p - pbeg;
       if (plane_exists(p) && !mbar_wait_bounded(&bars[(unsigned)lp % kLNS], ((unsigned)lp / kLNS) & 1u, a.timeout_ns))
-        s_fail = 1;
+        atomicOr((int *)wfail, 2);
     }
-    __syncthreads();
-    if (s_fail) return false;
+    if (pfail) atomicOr((int *)wfail, 2);
+    wg_bar(wg);
+    if (*wfail) return false;
     if (p > waited) waited = p;
     return true;
   };
   if (tid == 0)
-    for (int p = pbeg; p <= pbeg + 3; p++) issue(p);
+    for (int p = pbeg; p <= pbeg + kLNS - 1; p++) issue(p);
 
   const int r = tid >> 5, s = tid & 31;  // row y0 + r, half-row cell j0 + s
   const int y = y0 + r, jb = 4 + s, j = j0 + s;
@@ -925,16 +1028,18 @@ __global__ void __launch_bounds__(kThreads, 2) k_learned_pass(ModelDev m, Learne
 #pragma unroll
   for (int q = 0; q < kPartials; q++) dacc[q] = 0.0;
   bool ok = wait_plane(z0 - 1) && wait_plane(z0);
-  bool tc_ok = true;
   Vec3 pd{0.f, 0.f, 0.f};  // -z neighbour: plane k - 1, cell jb, this step's parity
-  if (ok && plane_exists(z0 - 1)) {
-    const float *q0 = slot_ptr(z0 - 1) + ((r + 1) * 2 + ((colour + y + z0) & 1)) * HALF + jb;
-    pd = Vec3{q0[0], q0[kLPF], q0[2 * kLPF]};
+  if (ok) {
+    if (plane_exists(z0 - 1)) {
+      const float *q0 = slot_ptr(z0 - 1) + ((r + 1) * 2 + ((colour + y + z0) & 1)) * HALF + jb;
+      pd = Vec3{q0[0], q0[kLPF], q0[2 * kLPF]};
+    }
+    release(z0 - 1);
   }
   for (int k = z0; ok && k < z1; k++) {
     ok = wait_plane(k + 1);
     if (!ok) break;
-    if (tid == 0) issue(k + 3);
+    if (tid == 0 && !issue(k + kLNS - 1)) pfail = true;
     const int h = (colour + y + k) & 1;
     const int x = 2 * j + h;
     const bool valid = live_row && x < nx;
@@ -958,13 +1063,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_learned_pass(ModelDev m, Learne
     for (int d = 0; d < 6; d++)  // an absent neighbour is the zero vector, as the gathering kernel has it
       if (w[d] == 0.f) nb[d] = Vec3{0.f, 0.f, 0.f};
     pd = h ? xm : xp;  // the other-parity cell jb of plane k: the next step's -z neighbour
+    release(k);         // plane k is not read again (plane k + 1, read above, is released at the next step)
     float f[kIn] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     if (valid) site_features(nb, w, St.T, f);
     float o[kOut];
-    if (!cta_mlp_tc(T, phase, a.timeout_ns, f, o)) {  // CTA-uniform
-      tc_ok = false;
-      break;
-    }
+    if (!wg_mlp_tc(T, &s_mma[wg], wfail, phase, a.timeout_ns, f, o)) break;  // warpgroup-uniform
     if (!valid) continue;
     int sid = -1;
     float sz = 0.f;
@@ -1011,9 +1114,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_learned_pass(ModelDev m, Learne
       dacc[9] += (double)nf.z;
     }
   }
-  if (!ok || !tc_ok) {
+  __syncthreads();  // both warpgroups have left the plane loop
+  const int fl = s_wfail[0] | s_wfail[1];
+  if (fl) {
     if (tid == 0) {
-      atomicOr(a.err, ok ? 1u : 2u);
+      atomicOr(a.err, (fl & 2) ? 2u : 1u);
       for (int q = max(waited + 1, last_issued - kLNS + 1); q <= last_issued; q++) {
         if (!plane_exists(q)) continue;
         const int lp = q - pbeg;
