@@ -127,9 +127,9 @@ int mcl_get_sweep_counter(mcl_engine *e, unsigned long long *sweep);
  * after enqueueing; errors of the device work surface at the next synchronising call. */
 int mcl_sweeps(mcl_engine *e, int n, int measure);
 /* One step of a caller's measurement loop in one call and one host synchronisation: T (n_replicas floats, or
- * null to keep the temperatures) goes up through pinned staging, n measured sweeps run as mcl_sweeps(e, n, 1),
- * and their records come down into out[s * n_replicas + r] (sweep s, replica r), together with the kernels'
- * error words. The same as mcl_set_temperature per replica, mcl_sweeps and mcl_read_series (the loop of
+ * null to keep the temperatures) goes up, n measured sweeps run as mcl_sweeps(e, n, 1), and their records come
+ * down into out[s * n_replicas + r] (sweep s, replica r), together with the kernels' error words. Both directions
+ * pass through the engine's mapped pinned staging, moved by two small kernels on the engine's stream. The same as mcl_set_temperature per replica, mcl_sweeps and mcl_read_series (the loop of
  * src/evolve_thermal.cu:78-106), without their separate round trips. */
 int mcl_sweeps_io(mcl_engine *e, int n, const float *T, mcl_observables *out);
 /* Number of records in the series; reading copies them to the host (synchronises). */

@@ -647,7 +647,7 @@ int mcl_sweeps_io(mcl_engine *e, int n, const float *T, mcl_observables *out) {
     for (int r = 0; r < e->n_rep; r++)
       if (!(T[r] >= 0.f) || !isfinite(T[r]))
         return fail(MCL_ERR_ARG, "temperature of replica %d must be finite and >= 0 (got %g)", r, T[r]);
-  // pinned staging: two error words, the temperatures, the records (64-byte aligned parts)
+  // mapped pinned staging: two error words, the temperatures, the records (64-byte aligned parts)
   const size_t t_off = 64, rec_off = t_off + ((size_t)e->n_rep * sizeof(float) + 63) / 64 * 64;
   const size_t rec_bytes = (size_t)n * e->n_rep * sizeof(ObsRecord), need = rec_off + rec_bytes;
   if (e->io_inflight || need > e->h_io_bytes) CK(cudaStreamSynchronize(e->stream));
@@ -655,27 +655,30 @@ int mcl_sweeps_io(mcl_engine *e, int n, const float *T, mcl_observables *out) {
   if (need > e->h_io_bytes) {
     cudaFreeHost(e->h_io);
     e->h_io = nullptr;
+    e->d_io = nullptr;
     e->h_io_bytes = 0;
-    CK(cudaHostAlloc(&e->h_io, need, cudaHostAllocDefault));
+    CK(cudaHostAlloc(&e->h_io, need, cudaHostAllocMapped));
+    CK(cudaHostGetDevicePointer(&e->d_io, e->h_io, 0));
     e->h_io_bytes = need;
   }
   unsigned *words = (unsigned *)e->h_io;
   float *hT = (float *)((char *)e->h_io + t_off);
   ObsRecord *rec = (ObsRecord *)((char *)e->h_io + rec_off);
+  char *dio = (char *)e->d_io;
   words[0] = words[1] = 0;
   if (T) {
     memcpy(hT, T, (size_t)e->n_rep * sizeof(float));
     e->io_inflight = true;
-    CK(cudaMemcpy2DAsync((char *)e->d_state + offsetof(RepState, T), sizeof(RepState), hT, sizeof(float),
-                         sizeof(float), e->n_rep, cudaMemcpyHostToDevice, e->stream));
+    CK(launch_io_in(e->stream, e->d_state, (const float *)(dio + t_off), e->n_rep));
+    e->launches++;
   }
   const int first = e->series_len;
   int rc = mcl_sweeps(e, n, 1);
   if (rc) return rc;
   e->io_inflight = true;
-  CK(cudaMemcpyAsync(rec, e->d_series + (size_t)first * e->n_rep, rec_bytes, cudaMemcpyDeviceToHost, e->stream));
-  if (unsigned *w = fused_error_word(e)) CK(cudaMemcpyAsync(&words[0], w, sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream));
-  if (e->d_lerr) CK(cudaMemcpyAsync(&words[1], e->d_lerr, sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream));
+  CK(launch_io_out(e->stream, e->d_series, first, n, e->n_rep, (ObsRecord *)(dio + rec_off), fused_error_word(e),
+                   e->d_lerr, (unsigned *)dio));
+  e->launches++;
   CK(cudaStreamSynchronize(e->stream));
   e->io_inflight = false;
   if ((rc = fused_report_error(e, words[0]))) return rc;

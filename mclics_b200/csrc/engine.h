@@ -82,7 +82,8 @@ struct mcl_engine {
   cudaGraphExec_t graph[2] = {nullptr, nullptr};  // [measure]: the sweeps of one replay, from buffer graph_cur
   int graph_cur[2] = {0, 0};
   const void *graph_series = nullptr;             // series buffer the measuring graph writes
-  void *h_io = nullptr;      // pinned staging of mcl_sweeps_io: error words, temperatures, observables records
+  void *h_io = nullptr;      // mapped pinned staging of mcl_sweeps_io: error words, temperatures, observables records
+  void *d_io = nullptr;      // its device address
   size_t h_io_bytes = 0;
   bool io_inflight = false;  // copies that read or write h_io may still be queued (an error return before the sync)
 

@@ -401,6 +401,38 @@ cudaError_t launch_zslab_planes(const LaunchCtx &c, float *dir, float *lo, float
   return cudaGetLastError();
 }
 
+// Step input and output of mcl_sweeps_io through mapped pinned host memory (no copy-engine round trips): the
+// replicas' temperatures in; the records of series rows first_row .. first_row + n_rows - 1 and the two error words
+// out. The caller validates the row range against the series it has written.
+__global__ void k_io_in(RepState *__restrict__ st, const float *__restrict__ host_T, int n_rep) {
+  for (int r = threadIdx.x; r < n_rep; r += blockDim.x) st[r].T = host_T[r];
+}
+
+__global__ void k_io_out(const ObsRecord *__restrict__ series, long long first_row, int n_rows, int n_rep,
+                         ObsRecord *__restrict__ host_rec, const unsigned *__restrict__ err0,
+                         const unsigned *__restrict__ err1, unsigned *__restrict__ host_words) {
+  static_assert(sizeof(ObsRecord) % 8 == 0, "records move as 8-byte words");
+  const long long words = (long long)n_rows * n_rep * (long long)(sizeof(ObsRecord) / 8);
+  const unsigned long long *src = reinterpret_cast<const unsigned long long *>(series + first_row * n_rep);
+  unsigned long long *dst = reinterpret_cast<unsigned long long *>(host_rec);
+  for (long long i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
+  if (threadIdx.x == 0) {
+    host_words[0] = err0 ? *err0 : 0u;
+    host_words[1] = err1 ? *err1 : 0u;
+  }
+}
+
+cudaError_t launch_io_in(cudaStream_t stream, RepState *st, const float *host_T, int n_rep) {
+  k_io_in<<<1, 32, 0, stream>>>(st, host_T, n_rep);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_io_out(cudaStream_t stream, const ObsRecord *series, long long first_row, int n_rows, int n_rep,
+                          ObsRecord *host_rec, const unsigned *err0, const unsigned *err1, unsigned *host_words) {
+  k_io_out<<<1, kThreads, 0, stream>>>(series, first_row, n_rows, n_rep, host_rec, err0, err1, host_words);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_refresh_ghosts(const LaunchCtx &c, int max_ny_nz, int max_px_nz) {
   const int bx = 148;
   k_ghosts_x<<<dim3(bx, c.n_replicas), kThreads, 0, c.stream>>>(c.reps, c.n_replicas, c.dir);
