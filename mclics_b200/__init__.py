@@ -280,20 +280,27 @@ class Engine:
 
     def sweeps_io(self, n, T=None, out=None):
         """n measured sweeps in one call: T (one float32 per replica, or None to keep the temperatures) goes up, the
-        n x replicas observables records come back (in `out` when given, an OBS_DTYPE array of that size)."""
+        n x replicas observables records come back (in `out` when given, an OBS_DTYPE array of that size).
+        The data addresses of the last T and out arrays are cached while this engine holds them (numpy refuses to
+        resize an array that another object references, so the addresses stay valid)."""
         n_rep = self.n
         if out is None:
             out = np.zeros(n * n_rep, OBS_DTYPE)
         elif out.dtype != OBS_DTYPE or out.size < n * n_rep or not out.flags.c_contiguous:
             raise ValueError(f"out must be a contiguous OBS_DTYPE array of at least {n * n_rep} records")
+        cache = self.__dict__.setdefault("_io_cache", [None, 0, None, 0])
         tp = None
         if T is not None:
-            if not (isinstance(T, np.ndarray) and T.dtype == np.float32 and T.flags.c_contiguous):
-                T = np.ascontiguousarray(T, dtype=np.float32)
-            if T.size != n_rep:
-                raise ValueError(f"T needs {n_rep} values, got {T.size}")
-            tp = T.ctypes.data
-        check(lib().mcl_sweeps_io(self._h, n, tp, out.ctypes.data))
+            if T is not cache[0]:
+                if not (isinstance(T, np.ndarray) and T.dtype == np.float32 and T.flags.c_contiguous):
+                    T = np.ascontiguousarray(T, dtype=np.float32)
+                if T.size != n_rep:
+                    raise ValueError(f"T needs {n_rep} values, got {T.size}")
+                cache[0], cache[1] = T, T.ctypes.data
+            tp = cache[1]
+        if out is not cache[2]:
+            cache[2], cache[3] = out, out.ctypes.data
+        check(lib().mcl_sweeps_io(self._h, n, tp, cache[3]))
         return out
 
     def series_length(self):
