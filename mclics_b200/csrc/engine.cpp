@@ -133,6 +133,9 @@ static void drop_graphs(mcl_engine *e) {
     e->graph[m] = nullptr;
   }
   e->graph_series = nullptr;
+  if (e->graph_io) cudaGraphExecDestroy(e->graph_io);
+  e->graph_io = nullptr;
+  e->graph_io_series = e->graph_io_stage = nullptr;
 }
 
 // Sweeps per captured graph: one for the in-place colour passes, two for the ping-pong fused kernel (one per
@@ -666,19 +669,59 @@ int mcl_sweeps_io(mcl_engine *e, int n, const float *T, mcl_observables *out) {
   ObsRecord *rec = (ObsRecord *)((char *)e->h_io + rec_off);
   char *dio = (char *)e->d_io;
   words[0] = words[1] = 0;
-  if (T) {
+  int rc;
+  // One measured sweep of a colour-pass plan with graphs on: the whole step is one captured graph (input kernel,
+  // the sweep's kernels, output kernel reading the newest record), captured again when a buffer it uses moves.
+  const bool use_fused = e->fused && !e->record_dec && !e->d_mlp;
+  if (T && n == 1 && use_fused && e->use_graphs && !e->profile && fused_is_pass_plan(e)) {
+    if ((rc = ensure_series(e, e->series_len + 1))) return rc;
+    if ((rc = refresh_ghosts(e))) return rc;
+    if (!e->graph_io || e->graph_io_series != (const void *)e->d_series || e->graph_io_stage != e->d_io) {
+      if (e->graph_io) cudaGraphExecDestroy(e->graph_io);
+      e->graph_io = nullptr;
+      cudaGraph_t g = nullptr;
+      CK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+      const long long l0 = e->launches;
+      cudaError_t ce = launch_io_in(e->stream, e->d_state, (const float *)(dio + t_off), e->n_rep);
+      rc = ce == cudaSuccess ? fused_sweep(e, true, nullptr, nullptr) : MCL_OK;
+      if (ce == cudaSuccess && !rc)
+        ce = launch_io_out(e->stream, e->d_series, 0, e->d_series_len, 1, e->n_rep, (ObsRecord *)(dio + rec_off),
+                           fused_error_word(e), e->d_lerr, (unsigned *)dio);
+      const cudaError_t ee = cudaStreamEndCapture(e->stream, &g);
+      e->launches = l0;
+      if (rc || ce != cudaSuccess || ee != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        if (rc) return rc;
+        return cuda_fail(ce != cudaSuccess ? ce : ee, "mcl_sweeps_io: graph capture");
+      }
+      const cudaError_t ie = cudaGraphInstantiate(&e->graph_io, g, 0);
+      cudaGraphDestroy(g);
+      if (ie != cudaSuccess) {
+        e->graph_io = nullptr;
+        return cuda_fail(ie, "cudaGraphInstantiate");
+      }
+      e->graph_io_series = e->d_series;
+      e->graph_io_stage = e->d_io;
+    }
     memcpy(hT, T, (size_t)e->n_rep * sizeof(float));
     e->io_inflight = true;
-    CK(launch_io_in(e->stream, e->d_state, (const float *)(dio + t_off), e->n_rep));
+    CK(cudaGraphLaunch(e->graph_io, e->stream));
+    e->launches += 2 + fused_launches_per_sweep(e);
+    e->series_len++;
+  } else {
+    if (T) {
+      memcpy(hT, T, (size_t)e->n_rep * sizeof(float));
+      e->io_inflight = true;
+      CK(launch_io_in(e->stream, e->d_state, (const float *)(dio + t_off), e->n_rep));
+      e->launches++;
+    }
+    const int first = e->series_len;
+    if ((rc = mcl_sweeps(e, n, 1))) return rc;
+    e->io_inflight = true;
+    CK(launch_io_out(e->stream, e->d_series, first, nullptr, n, e->n_rep, (ObsRecord *)(dio + rec_off),
+                     fused_error_word(e), e->d_lerr, (unsigned *)dio));
     e->launches++;
   }
-  const int first = e->series_len;
-  int rc = mcl_sweeps(e, n, 1);
-  if (rc) return rc;
-  e->io_inflight = true;
-  CK(launch_io_out(e->stream, e->d_series, first, n, e->n_rep, (ObsRecord *)(dio + rec_off), fused_error_word(e),
-                   e->d_lerr, (unsigned *)dio));
-  e->launches++;
   CK(cudaStreamSynchronize(e->stream));
   e->io_inflight = false;
   if ((rc = fused_report_error(e, words[0]))) return rc;
@@ -789,6 +832,14 @@ int mcl_debug_wait_limit(mcl_engine *e, long long timeout_ns, int withhold_first
   drop_graphs(e);
   if (!e->fused) return fail(MCL_ERR_STATE, "this engine does not use the fused tiled sweep");
   fused_set_test_hooks(e, timeout_ns, withhold_first_load);
+  return MCL_OK;
+}
+
+int mcl_set_adaptation(mcl_engine *e, int enable) {
+  if (!e) return fail(MCL_ERR_ARG, "null engine");
+  CK(cudaStreamSynchronize(e->stream));
+  e->adapt = enable != 0;
+  drop_graphs(e);  // captured finalisations hold the flag as an argument
   return MCL_OK;
 }
 

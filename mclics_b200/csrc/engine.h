@@ -82,6 +82,8 @@ struct mcl_engine {
   cudaGraphExec_t graph[2] = {nullptr, nullptr};  // [measure]: the sweeps of one replay, from buffer graph_cur
   int graph_cur[2] = {0, 0};
   const void *graph_series = nullptr;             // series buffer the measuring graph writes
+  cudaGraphExec_t graph_io = nullptr;  // mcl_sweeps_io's step (input kernel, one measured sweep, output kernel)
+  const void *graph_io_series = nullptr, *graph_io_stage = nullptr;  // the buffers it was captured with
   void *h_io = nullptr;      // mapped pinned staging of mcl_sweeps_io: error words, temperatures, observables records
   void *d_io = nullptr;      // its device address
   size_t h_io_bytes = 0;

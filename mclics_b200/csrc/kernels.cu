@@ -408,10 +408,13 @@ __global__ void k_io_in(RepState *__restrict__ st, const float *__restrict__ hos
   for (int r = threadIdx.x; r < n_rep; r += blockDim.x) st[r].T = host_T[r];
 }
 
-__global__ void k_io_out(const ObsRecord *__restrict__ series, long long first_row, int n_rows, int n_rep,
-                         ObsRecord *__restrict__ host_rec, const unsigned *__restrict__ err0,
+// series_len non-null (a captured graph, whose arguments are fixed): the rows are the newest n_rows, and first_row is
+// ignored.
+__global__ void k_io_out(const ObsRecord *__restrict__ series, long long first_row, const int *__restrict__ series_len,
+                         int n_rows, int n_rep, ObsRecord *__restrict__ host_rec, const unsigned *__restrict__ err0,
                          const unsigned *__restrict__ err1, unsigned *__restrict__ host_words) {
   static_assert(sizeof(ObsRecord) % 8 == 0, "records move as 8-byte words");
+  if (series_len) first_row = max(0, *series_len - n_rows);
   const long long words = (long long)n_rows * n_rep * (long long)(sizeof(ObsRecord) / 8);
   const unsigned long long *src = reinterpret_cast<const unsigned long long *>(series + first_row * n_rep);
   unsigned long long *dst = reinterpret_cast<unsigned long long *>(host_rec);
@@ -427,9 +430,11 @@ cudaError_t launch_io_in(cudaStream_t stream, RepState *st, const float *host_T,
   return cudaGetLastError();
 }
 
-cudaError_t launch_io_out(cudaStream_t stream, const ObsRecord *series, long long first_row, int n_rows, int n_rep,
-                          ObsRecord *host_rec, const unsigned *err0, const unsigned *err1, unsigned *host_words) {
-  k_io_out<<<1, kThreads, 0, stream>>>(series, first_row, n_rows, n_rep, host_rec, err0, err1, host_words);
+cudaError_t launch_io_out(cudaStream_t stream, const ObsRecord *series, long long first_row, const int *series_len,
+                          int n_rows, int n_rep, ObsRecord *host_rec, const unsigned *err0, const unsigned *err1,
+                          unsigned *host_words) {
+  k_io_out<<<1, kThreads, 0, stream>>>(series, first_row, series_len, n_rows, n_rep, host_rec, err0, err1,
+                                       host_words);
   return cudaGetLastError();
 }
 

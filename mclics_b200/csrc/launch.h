@@ -44,10 +44,12 @@ cudaError_t launch_observe(const LaunchCtx &c, int geo, const BlockTable &sites,
 // caller's buffers of 3 py px floats each; a null buffer skips its side.
 cudaError_t launch_zslab_planes(const LaunchCtx &c, float *dir, float *lo, float *hi, int pack);
 // mcl_sweeps_io's step input (temperatures from mapped host memory into the replicas' state) and output (series rows
-// first_row .. first_row + n_rows - 1 and the error words, null for absent ones, into mapped host memory).
+// first_row .. first_row + n_rows - 1, or with series_len the newest n_rows, and the error words, null for absent
+// ones, into mapped host memory).
 cudaError_t launch_io_in(cudaStream_t stream, RepState *st, const float *host_T, int n_rep);
-cudaError_t launch_io_out(cudaStream_t stream, const ObsRecord *series, long long first_row, int n_rows, int n_rep,
-                          ObsRecord *host_rec, const unsigned *err0, const unsigned *err1, unsigned *host_words);
+cudaError_t launch_io_out(cudaStream_t stream, const ObsRecord *series, long long first_row, const int *series_len,
+                          int n_rows, int n_rep, ObsRecord *host_rec, const unsigned *err0, const unsigned *err1,
+                          unsigned *host_words);
 // Per-replica sums of the partials over a block table and the accepted rotations (kZslabSums doubles each).
 cudaError_t launch_item_sums(const LaunchCtx &c, const BlockTable &items, const double *partials, int measure,
                              double *out);

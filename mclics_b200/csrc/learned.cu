@@ -1322,12 +1322,6 @@ int mcl_set_proposal(mcl_engine *e, const mcl_mlp *mlp, float kappa_max) {
   return MCL_OK;
 }
 
-int mcl_set_adaptation(mcl_engine *e, int enable) {
-  if (!e) return fail(MCL_ERR_ARG, "null engine");
-  e->adapt = enable != 0;
-  return MCL_OK;
-}
-
 int mcl_extract_samples(mcl_engine *e, int replica, long long n, unsigned long long seed, float *d_features,
                         float *d_directors) {
   if (!e) return fail(MCL_ERR_ARG, "null engine");

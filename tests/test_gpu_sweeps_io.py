@@ -90,3 +90,32 @@ def test_sweeps_io_refuses_bad_arguments_and_stays_usable():
     assert recs.size == 4 and np.all(np.isfinite(recs["energy"])) and np.all(recs["n_valid"] == 16 ** 3)
     assert recs["sweep"][0] == recs["sweep"][1] and recs["sweep"][2] == recs["sweep"][3] > recs["sweep"][0]
     e.close()
+
+
+@pytest.mark.parametrize("io", [False, True], ids=["sweeps", "sweeps_io"])
+def test_adaptation_switch_reaches_captured_graphs(io):
+    """ang_var adaptation is an argument of the captured finalisation: switching it off after a graph was captured
+    must stop the adaptation in the graph replays too (mcl_sweeps and mcl_sweeps_io's one-step graph)."""
+    e = make(M.Model("ll"), [16])
+    e.set_graphs(True)
+    T = np.array([1.0], np.float32)
+
+    def run(k):
+        if io:
+            for _ in range(k):
+                e.sweeps_io(1, T)
+        else:
+            e.sweeps(k, measure=True)
+
+    run(4)  # captures with adaptation on
+    a0 = e.ang_var(0)
+    run(4)
+    assert e.ang_var(0) != a0  # adapting
+    e.set_adaptation(False)
+    a1 = e.ang_var(0)
+    run(6)
+    assert e.ang_var(0) == a1
+    e.set_adaptation(True)
+    run(4)
+    assert e.ang_var(0) != a1
+    e.close()
