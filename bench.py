@@ -124,7 +124,7 @@ def measured_peaks():
 
 def ncu_traffic(workload, tile_config):
     """Per-launch DRAM bytes of the sweep kernel from the committed ncu summary (profiles/ncu_traffic.json), when
-    the summary was taken with the same kernel kind (colour passes: tile configurations 2-5) as this run."""
+    the summary was taken with the same kernel kind (colour passes: tile configurations 2-6) as this run."""
     p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if not os.path.exists(p):
         return None
@@ -284,6 +284,9 @@ def gpu_arm(args, rank, world, local_rank):
         tuning = dict(eng.plan(), candidates=0)
     else:
         tuning = eng.autotune(3)
+    # every record the timed regions append (device steps, profiled sweeps, two end-to-end loops with warm-up)
+    # fits the series, so no timed sweep reallocates it or captures its graph again
+    eng.reserve_series(eng.series_length() + 4 * args.steps + 256)
     eng.set_graphs(True)
     eng.sweeps(2, measure=True)  # captures the graph outside the timed region
     eng.synchronize()

@@ -89,6 +89,7 @@ def lib():
             "mcl_sweeps_io": [vp, i, vp, vp],
             "mcl_series_length": [vp, P(i)],
             "mcl_read_series": [vp, i, i, i, vp],
+            "mcl_reserve_series": [vp, i],
             "mcl_clear_series": [vp],
             "mcl_measure": [vp, i, P(CObservables)],
             "mcl_synchronize": [vp],
@@ -315,6 +316,9 @@ class Engine:
         if count:
             check(lib().mcl_read_series(self._h, r, first, count, out.ctypes.data))
         return out
+
+    def reserve_series(self, rows):
+        check(lib().mcl_reserve_series(self._h, rows))
 
     def clear_series(self):
         check(lib().mcl_clear_series(self._h))

@@ -796,6 +796,14 @@ int mcl_read_series(mcl_engine *e, int replica, int first, int count, mcl_observ
   return MCL_OK;
 }
 
+int mcl_reserve_series(mcl_engine *e, int rows) {
+  if (!e) return fail(MCL_ERR_ARG, "null engine");
+  if (rows < 0) return fail(MCL_ERR_ARG, "mcl_reserve_series: negative row count");
+  if (rows <= e->series_cap) return MCL_OK;
+  drop_graphs(e);  // captured graphs write the old buffer
+  return ensure_series(e, rows);
+}
+
 int mcl_clear_series(mcl_engine *e) {
   if (!e) return fail(MCL_ERR_ARG, "null engine");
   CK(cudaMemsetAsync(e->d_series_len, 0, sizeof(int), e->stream));

@@ -119,3 +119,27 @@ def test_adaptation_switch_reaches_captured_graphs(io):
     run(4)
     assert e.ang_var(0) != a1
     e.close()
+
+
+def test_reserved_series_keeps_the_records():
+    """mcl_reserve_series sizes the series once; the records and directors of the sweeps that follow are those of an
+    engine that grows its series as it goes (graphs on, so a reallocation also means a new capture)."""
+    a, b = make(M.Model("ll"), [16, 20]), make(M.Model("ll"), [16, 20])
+    for e in (a, b):
+        e.set_graphs(True)
+    a.reserve_series(500)
+    a.reserve_series(10)  # smaller than the capacity: nothing changes
+    T = np.array([0.9, 1.1], np.float32)
+    for _ in range(3):
+        a.sweeps(70, measure=True)
+        b.sweeps(70, measure=True)
+        ra, rb = a.sweeps_io(1, T), b.sweeps_io(1, T)
+        assert ra.tobytes() == rb.tobytes()
+    assert a.series_length() == b.series_length() == 213
+    for r in range(2):
+        assert a.series(r).tobytes() == b.series(r).tobytes()
+        assert np.array_equal(a.download(r), b.download(r))
+    with pytest.raises(M.McLicsError):
+        a.reserve_series(-1)
+    a.close()
+    b.close()
