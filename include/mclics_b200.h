@@ -137,7 +137,8 @@ int mcl_series_length(mcl_engine *e, int *n);
 int mcl_read_series(mcl_engine *e, int replica, int first, int count, mcl_observables *out);
 int mcl_clear_series(mcl_engine *e);
 /* Sizes the series for `rows` records per replica, so that the sweeps appending them neither reallocate it (an
- * allocation and a host synchronisation) nor capture their graphs again. */
+ * allocation and a host synchronisation) nor capture their graphs again. No counterpart in the reference, which
+ * keeps no series (its loops fold each record into running sums, src/evolve_thermal.cu:84-95). */
 int mcl_reserve_series(mcl_engine *e, int rows);
 /* Observables of the current state (synchronises). acceptance/ang_var fields refer to the last sweep. */
 int mcl_measure(mcl_engine *e, int replica, mcl_observables *out);
