@@ -98,7 +98,9 @@ typedef struct mcl_observables {
 
 typedef struct mcl_engine mcl_engine;
 
-/* Creates an engine on the current CUDA device holding n_replicas lattices. Directors start at (0, 0, 1). */
+/* Creates an engine on the current CUDA device holding n_replicas lattices. Directors start at (0, 0, 1). In place
+ * of the EvolveNGPU constructor (include/evolve.cuh:22-42) and the device allocations and RNG set-up at the start
+ * of its run() (src/evolve_thermal.cu:48-66); mcl_destroy releases what the reference never frees. */
 int mcl_create(const mcl_model *model, const mcl_replica *replicas, int n_replicas, int schedule,
                mcl_engine **out);
 int mcl_destroy(mcl_engine *e);
@@ -112,12 +114,16 @@ int mcl_set_geometry(mcl_engine *e, int replica, const int *pt, const float *nor
 int mcl_upload_directors(mcl_engine *e, int replica, const float *ni);
 int mcl_download_directors(mcl_engine *e, int replica, float *ni);
 
-/* Per-replica parameters; replica = -1 applies to all. */
+/* Per-replica parameters; replica = -1 applies to all. T is the temperature the mode loops copy to the device
+ * (src/evolve_thermal.cu:80), elecE the field magnitude the electric mode sweeps (src/evolve_electric.cu:80-82),
+ * ang_var the rotation amplitude Monte_Carlo_Step_GPU adapts (src/evolve.cu:302-313, starting at 0.5 per run,
+ * src/evolve_thermal.cu:43). */
 int mcl_set_temperature(mcl_engine *e, int replica, float T);
 int mcl_set_field(mcl_engine *e, int replica, float elecE);
 int mcl_set_ang_var(mcl_engine *e, int replica, float ang_var);
 int mcl_get_ang_var(mcl_engine *e, int replica, float *ang_var);
-/* Global sweep counter (the Philox counter of the next sweep). */
+/* Global sweep counter (the Philox counter of the next sweep). No counterpart: the reference advances per-box
+ * XORWOW states instead (src/evolve.cu:35-41). */
 int mcl_set_sweep_counter(mcl_engine *e, unsigned long long sweep);
 int mcl_get_sweep_counter(mcl_engine *e, unsigned long long *sweep);
 
@@ -145,23 +151,26 @@ int mcl_measure(mcl_engine *e, int replica, mcl_observables *out);
 int mcl_synchronize(mcl_engine *e);
 
 /* Records one byte per site for the sweeps that follow (bit 0: rotation accepted, bit 1: flip accepted,
- * bit 7: site visited); mcl_read_decisions copies those of the last sweep. Test hook for the replay harness. */
+ * bit 7: site visited); mcl_read_decisions copies those of the last sweep. Test hook for the replay harness (no
+ * counterpart in the reference). */
 int mcl_record_decisions(mcl_engine *e, int enable);
 int mcl_read_decisions(mcl_engine *e, int replica, unsigned char *out);
 
 /* Work of this engine goes to `stream` (a cudaStream_t of the current device; NULL restores the engine's own
- * stream), so a caller can order it with its own work and time it with its own events. */
+ * stream), so a caller can order it with its own work and time it with its own events. No counterpart (the
+ * reference uses the default stream). */
 int mcl_set_stream(mcl_engine *e, void *stream);
 /* Kernel timing: with enable != 0 every following sweep records CUDA events around its sweep kernel(s) (not the
  * per-sweep finalisation); mcl_profile_read returns their total time in ms and the number of sweeps timed, and
- * the number of kernels this engine has launched since creation. */
+ * the number of kernels this engine has launched since creation. No counterpart in the reference. */
 int mcl_profile(mcl_engine *e, int enable);
 int mcl_profile_read(mcl_engine *e, double *sweep_kernel_ms, long long *timed_sweeps, long long *kernel_launches);
 
 /* Failure-detection test hook: every wait of the fused tiled sweep on a TMA copy gives up after timeout_ns
  * (> 0 to change; default 2 s) and the sweep then reports MCL_ERR_CUDA at the next synchronising call, with
  * the context still usable. With withhold_first_load != 0 each CTA leaves its first copy unissued, so that
- * wait runs out; 0 restores normal operation. MCL_ERR_STATE if the engine does not use the fused sweep. */
+ * wait runs out; 0 restores normal operation. MCL_ERR_STATE if the engine does not use the fused sweep. No
+ * counterpart in the reference. */
 int mcl_debug_wait_limit(mcl_engine *e, long long timeout_ns, int withhold_first_load);
 
 /* Runs a whole McLics input file in the current directory, like the reference program with a *GPU evolution
@@ -214,7 +223,8 @@ typedef struct mcl_tuning {
 } mcl_tuning;
 int mcl_autotune(mcl_engine *e, int trial_sweeps, mcl_tuning *out);
 /* Applies a plan (e.g. one mcl_autotune chose earlier) without timing: planes_per_segment <= 0 lets the heuristic
- * choose. mcl_get_plan fills the plan fields of *out (tile_config .. work_items; the timing fields are 0). */
+ * choose. mcl_get_plan fills the plan fields of *out (tile_config .. work_items; the timing fields are 0). No
+ * counterpart in the reference, whose launch shape is fixed (src/evolve.cu:335-339, 409-410). */
 int mcl_set_plan(mcl_engine *e, int tile_config, int planes_per_segment);
 int mcl_get_plan(mcl_engine *e, mcl_tuning *out);
 
