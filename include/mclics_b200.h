@@ -294,7 +294,7 @@ int mcl_mlp_forward(const mcl_mlp *mlp, const float *d_features, long long n, fl
  * not arrive within 2 s (the CTA frees its tensor memory and stops). */
 int mcl_mlp_forward_tcgen05(const mcl_mlp *mlp, const float *d_features, long long n, float *d_out, void *stream);
 
-/* Training on the GPU: loss = -mean log(4 pi q(n | features)) over samples (maximum likelihood of the site's
+/* Training on the GPU (no counterpart in the reference): loss = -mean log(4 pi q(n | features)) over samples (maximum likelihood of the site's
  * conditional distribution), Adam (beta 0.9 / 0.999, eps 1e-8) on FP32 master weights, BF16-rounded weights in
  * the passes. Batches are device buffers in the mcl_extract_samples format, at most max_batch rows. */
 typedef struct mcl_trainer mcl_trainer;
