@@ -1,0 +1,31 @@
+"""bench.py --impl reference on the host cores: the reference's own CPU sweep + measurement (oracle/_ref) prints one
+JSON line with the keys the benchmark contract asks of the reference arm, on the same metric and workload as the
+GPU arm. Runs on CPU (one measured sweep of the 256^3 lattice); when oracle/_ref has not been built the arm must say
+so in an "unavailable" line and exit 0."""
+import json
+import os
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_reference_arm_prints_the_contract_line():
+    p = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "1", "--warmup", "1"],
+                       cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr[-2000:]
+    line = json.loads(p.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference"
+    if "unavailable" in line:
+        assert not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "mclics_ref_timing"))
+        return
+    for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+                "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert key in line, key
+    assert line["metric"] == "site-updates/s" and line["unit"] == "site-updates/s" and line["higher_is_better"]
+    assert line["config"]["workload"] == "ghrl_slab_256^3_k1:0.5:1.5_homeotropic_W1.5_T0.8"
+    assert line["value"] > 0 and line["steps"] == 1 and line["warmup"] == 1
+    cb = line["cpu_baseline"]
+    assert cb["kind"] == "reference" and cb["value"] == line["value"] and cb["cores"] >= 1 and cb["sample"]
+    assert line["e2e"] == {"value": line["value"], "unit": "site-updates/s", "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
