@@ -432,7 +432,7 @@ def learned_compare(args):
     the GPU from plain-sweep states (seed 3), then both proposals run the same number of measured sweeps from the
     same equilibrated start, and the integrated autocorrelation times of E and S (Sokal windowing) give effective
     samples per device second. The plain arm keeps ang_var fixed at its adapted value (the fixed-amplitude
-    judge)."""
+    proposal the learned one is measured against)."""
     import torch
     import mclics_b200 as M
     from mclics_b200 import analysis, learned

@@ -278,8 +278,8 @@ typedef struct mcl_mlp {
  * moves. Every site gets one learned trial per sweep, colour by colour (no separate n -> -n trial: the proposal is
  * symmetric under n -> -n). */
 int mcl_set_proposal(mcl_engine *e, const mcl_mlp *mlp, float kappa_max);
-/* ang_var adaptation after each sweep (default 1, as the reference). 0 keeps the plain proposal's amplitude fixed,
- * the fixed-amplitude judge of autocorrelation comparisons. */
+/* ang_var adaptation after each sweep (default 1, as the reference, src/evolve.cu:302-313). 0 keeps the plain
+ * proposal's amplitude fixed: the fixed-amplitude yardstick of autocorrelation comparisons. */
 int mcl_set_adaptation(mcl_engine *e, int enable);
 /* Training samples from the current state of one replica: n sites drawn with Philox(seed, sample index). Device
  * buffers: d_features n x 8 floats (7 features, then 1 for a non-empty site / 0 for an empty one), d_directors
