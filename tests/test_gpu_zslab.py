@@ -87,7 +87,7 @@ def test_slabs_reproduce_the_whole_lattice(case):
 def test_slab_engine_refuses_whole_lattice_calls():
     s = zslab.ZSlab(M.Model("ll"), 32, 16, 12, 0, 2, None, periodic_z=True, seed=3)
     for call in (lambda: s.eng.sweeps(1), lambda: s.eng.measure(0), lambda: s.eng.autotune(1),
-                 lambda: s.eng.set_plan(1, 0)):
+                 lambda: s.eng.set_plan(1, 0), lambda: s.eng.sweeps_io(1, np.array([1.0], np.float32))):
         with pytest.raises(M.McLicsError) as ei:
             call()
         assert ei.value.code == 4
