@@ -530,7 +530,9 @@ def main():
                     help="N > 1: split the workload's replicas across ranks (strong scaling) instead of one copy per rank")
     ap.add_argument("--learned", action="store_true",
                     help="learned vs plain proposal: train the proposal network, compare ESS/s of E and S")
-    ap.add_argument("--ess-sweeps", type=int, default=10000)
+    ap.add_argument("--ess-sweeps", type=int, default=120000,
+                    help="--learned: measured sweeps per arm (tau_S of the plain chain is 1500-2700 sweeps on c4, "
+                         "so shorter runs underestimate it)")
     ap.add_argument("--plan", default="",
                     help="tile configuration[,planes per z segment] instead of the autotuner (profiling runs)")
     ap.add_argument("--therm-sweeps", type=int, default=5000,
