@@ -22,9 +22,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
           "-I" + os.path.join(HERE, "..", "include")] + ARCH
 PER_FILE = {"kernels_ref8.cu": ["-fmad=false"]}
-SOURCES = ["kernels.cu", "kernels_ref8.cu", "sweep_fused.cu", "sweep_fused_ll.cu", "sweep_fused_ghrl.cu",
-           "sweep_fused_pear.cu", "sweep_pass_ll.cu", "sweep_pass_ghrl.cu", "sweep_pass_pear.cu", "observe_static.cu", "learned.cu", "extras.cu", "engine.cpp",
-           "driver.cpp"]
+SOURCES = ["sweep_pass_ghrl.cu", "sweep_pass_ghrl_chiral.cu", "sweep_pass_pear.cu", "sweep_pass_ll.cu",
+           "sweep_fused_ghrl.cu", "sweep_fused_pear.cu", "sweep_fused_ll.cu", "learned.cu", "kernels.cu",
+           "kernels_ref8.cu", "sweep_fused.cu", "observe_static.cu", "extras.cu", "engine.cpp", "driver.cpp"]  # slowest first: they start compiling first
 
 
 def nvcc():

@@ -9,6 +9,7 @@
 // multiple of 8 in x. For a periodic axis the cells x = -2, -1, nx, nx + 1 (likewise y) hold copies of the
 // wrapped sites ("ghosts"); the fused kernel reads them instead of wrapping. Padding beyond is zero.
 #pragma once
+#include <math.h>
 #include <stdint.h>
 
 namespace mcl {
@@ -84,37 +85,45 @@ __host__ __device__ inline long long dir_index(const RepDesc &r, int c, int x, i
 }
 
 // ---- Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11) ------------------------------------------------------
-// Counter (site, sweep_lo, sweep_hi, stream), key (seed_lo, seed_hi). Stream 0: plain move (u1 angle, u2 axis,
-// u3 rotation accept, u4 flip accept); stream 1: learned proposal; stream 2: initial conditions.
+// Every draw of this library uses a key fixed at compile time per stream and carries the seed in the counter:
+// counter (a, b, seed_lo, seed_hi + c_hi), key (kPhiloxKey0 + stream, kPhiloxKey1). Philox under one key is a
+// bijection of the 128-bit counter, so distinct (a, b, seed) give independent-looking blocks, and the ten round
+// keys are constants the compiler folds into the XORs (no per-call key schedule). Site draws use a = site,
+// b = sweep (low 32 bits), c_hi = sweep >> 32: two (seed, sweep) pairs share a counter only if their seeds differ
+// in the upper 32 bits by minus the difference of their sweep counts' upper 32 bits. Streams: 0 plain move
+// (u1 angle, u2 axis, u3 rotation accept, u4 flip accept), 1 learned proposal, 2 initial conditions, 3 training
+// samples.
 struct U4 {
   uint32_t x, y, z, w;
 };
+
+constexpr uint32_t kPhiloxKey0 = 0x694C634Du, kPhiloxKey1 = 0x30303242u;
 
 __host__ __device__ __forceinline__ U4 philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0,
                                                       uint32_t k1) {
 #pragma unroll
   for (int r = 0; r < 10; r++) {
-#ifdef __CUDA_ARCH__
-    uint32_t lo0 = 0xD2511F53u * c0, hi0 = __umulhi(0xD2511F53u, c0);
-    uint32_t lo1 = 0xCD9E8D57u * c2, hi1 = __umulhi(0xCD9E8D57u, c2);
-#else
-    uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
-    uint32_t lo0 = (uint32_t)p0, hi0 = (uint32_t)(p0 >> 32), lo1 = (uint32_t)p1, hi1 = (uint32_t)(p1 >> 32);
-#endif
-    uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+    const uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;  // one 32 x 32 -> 64 each
+    const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0, n2 = (uint32_t)(p0 >> 32) ^ c3 ^ k1;
+    c1 = (uint32_t)p1;
+    c3 = (uint32_t)p0;
     c0 = n0;
-    c1 = lo1;
     c2 = n2;
-    c3 = lo0;
     k0 += 0x9E3779B9u;
     k1 += 0xBB67AE85u;
   }
   return U4{c0, c1, c2, c3};
 }
 
+// One block of stream `stream` (a compile-time constant at every call site) at counter (a, b, seed, c_hi).
+__host__ __device__ __forceinline__ U4 stream_draws(uint32_t a, uint32_t b, unsigned long long seed, uint32_t c_hi,
+                                                     uint32_t stream) {
+  return philox4x32_10(a, b, (uint32_t)seed, (uint32_t)(seed >> 32) + c_hi, kPhiloxKey0 + stream, kPhiloxKey1);
+}
+
 __host__ __device__ __forceinline__ U4 site_draws(unsigned long long seed, unsigned long long sweep, uint32_t site,
                                                    uint32_t stream) {
-  return philox4x32_10(site, (uint32_t)sweep, (uint32_t)(sweep >> 32), stream, (uint32_t)seed, (uint32_t)(seed >> 32));
+  return stream_draws(site, (uint32_t)sweep, seed, (uint32_t)(sweep >> 32), stream);
 }
 
 // ---- draws of one site -----------------------------------------------------------------------------------
@@ -155,6 +164,32 @@ __host__ __device__ __forceinline__ float unif(uint32_t f, bool flip) {
 }
 __host__ __device__ __forceinline__ double unif_d(uint32_t f, bool flip) {
   return (double)f * (flip ? (1.0 / 16777216.0) : (1.0 / 2097152.0));
+}
+
+// Random initial director of one site (stream 2 of the site's Philox counter): successive draws (site, attempt)
+// give a point of the grid of odd integers in (-2^24, 2^24)^3; the first one strictly inside the ball of radius
+// 2^24 is projected onto the unit sphere. A uniform point of a ball projects to a uniform point of its sphere, and
+// the arithmetic is integer products, one IEEE double square root and IEEE double divisions, so host and device
+// give the same bits. An attempt is accepted with probability pi / 6; after 64 rejections (probability 1e-21) the
+// site takes (0, 0, 1).
+__host__ __device__ inline void random_director(unsigned long long seed, uint32_t site, float out[3]) {
+  for (uint32_t attempt = 0; attempt < 64; attempt++) {
+    const U4 r = site_draws(seed, attempt, site, 2);
+    const long long ix = 2ll * (long long)(r.x >> 8) + 1 - 16777216ll;
+    const long long iy = 2ll * (long long)(r.y >> 8) + 1 - 16777216ll;
+    const long long iz = 2ll * (long long)(r.z >> 8) + 1 - 16777216ll;
+    const long long s = ix * ix + iy * iy + iz * iz;  // < 3 * 2^48: exact
+    if (s < (1ll << 48)) {
+      const double len = sqrt((double)s);  // s < 2^48 is exact in double; sqrt rounds correctly
+      out[0] = (float)((double)ix / len);
+      out[1] = (float)((double)iy / len);
+      out[2] = (float)((double)iz / len);
+      return;
+    }
+  }
+  out[0] = 0.f;
+  out[1] = 0.f;
+  out[2] = 1.f;
 }
 
 // Rotation axis from the axis field exactly as `u2 < 0.333` / `u2 < 0.666` in double (src/evolve.cpp:156-160):

@@ -671,7 +671,7 @@ __global__ void k_extract_samples(const RepDesc *__restrict__ reps, const RepSta
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const RepDesc R = reps[rep];
-  const U4 u = philox4x32_10((uint32_t)i, (uint32_t)(i >> 32), 0u, 3u, (uint32_t)seed, (uint32_t)(seed >> 32));
+  const U4 u = stream_draws((uint32_t)i, (uint32_t)(i >> 32), seed, 0u, 3u);
   const unsigned long long N = (unsigned long long)R.nx * R.ny * R.nz;
   const unsigned long long site = (((unsigned long long)u.x << 32) | u.y) % N;
   const int x = (int)(site % R.nx);

@@ -143,8 +143,86 @@ __device__ __forceinline__ L acc_bond(const ModelDev &m, const V3<L> &x, const V
   return D == 0 ? mul_(w, u) : fma_(w, u, e);
 }
 
+// Lebwohl-Lasher sums: sum_j w_j (n.n_j)^2 over the six bonds, then one multiplication by -1.5 A (the bond
+// energy is that constant times a square, so it factors out of the sum).
+template <bool PXY, int D, typename L>
+__device__ __forceinline__ L ll_acc(const V3<L> &x, const V3<L> &y, const L &w, const L &s) {
+  const L b = dot(x, y);
+  if (PXY && D < 4) return D == 0 ? mul_(b, b) : fma_(b, b, s);
+  return D == 0 ? mul_(mul_(w, b), b) : fma_(mul_(w, b), b, s);
+}
+template <bool PXY, typename L>
+__device__ __forceinline__ L ll_sum(const ModelDev &m, const V3<L> &x, const V3<L> (&nb)[6], const L (&w)[6]) {
+  L s = ll_acc<PXY, 0>(x, nb[0], w[0], w[0]);
+  s = ll_acc<PXY, 1>(x, nb[1], w[1], s);
+  s = ll_acc<PXY, 2>(x, nb[2], w[2], s);
+  s = ll_acc<PXY, 3>(x, nb[3], w[3], s);
+  s = ll_acc<PXY, 4>(x, nb[4], w[4], s);
+  s = ll_acc<PXY, 5>(x, nb[5], w[5], s);
+  return mul_(splat<L>(-1.5f * m.A), s);
+}
+
+// GHRL without the chiral term as sums over the site's bonds. With a_i = n.r, a_j = n_j.r, b = n.n_j, the pair
+// energy of ghrl_bond is
+//   U = (1.5 a_i^2 + K) P + mu a_i a_j b + 1.5 nu b^2 + c0,   K = 1.5 a_j^2 - 1,   P = 1.5 rho b^2 + lambda - rho / 2,
+//   c0 = -mu / 9 - nu / 2,
+// so the site sums to sum_d [(A_a(d) + K_d) P_d + 1.5 nu B_d] + mu sum_a a_i,a (sum_{d on a} a_j,d b_d) + c0 sum_d w_d
+// (A_a = 1.5 a_i,a^2, B = b^2; an absent bond has w = 0, applied by scaling b and A + K). NS directors (1: one
+// site energy; 2: the old and new director of a trial) go through the bonds together, so each neighbour and its
+// K_d are used by both and then released.
+template <bool PXY, int NS, typename L>
+__device__ __forceinline__ void ghrl_sums(const ModelDev &m, const V3<L> *const (&x)[NS], const V3<L> (&nb)[6],
+                                          const L (&w)[6], L (&out)[NS]) {
+  const L h3 = splat<L>(1.5f), r15 = splat<L>(1.5f * m.rho), lamp = splat<L>(fmaf(-0.5f, m.rho, m.lam));
+  L e[NS], sB[NS];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    L A[NS], mab[NS];
+#pragma unroll
+    for (int i = 0; i < NS; i++) {
+      const L ai = a == 0 ? x[i]->x : (a == 1 ? x[i]->y : x[i]->z);
+      A[i] = mul_(mul_(h3, ai), ai);
+    }
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+      const int d = 2 * a + s;
+      const L aj = a == 0 ? nb[d].x : (a == 1 ? nb[d].y : nb[d].z);
+      const L K = fma_(mul_(h3, aj), aj, splat<L>(-1.f));
+#pragma unroll
+      for (int i = 0; i < NS; i++) {
+        L b = dot(*x[i], nb[d]), t = add_(A[i], K);
+        if (!(PXY && d < 4)) {
+          b = mul_(w[d], b);
+          t = mul_(w[d], t);
+        }
+        const L B = mul_(b, b), P = fma_(r15, B, lamp);
+        e[i] = d == 0 ? mul_(t, P) : fma_(t, P, e[i]);
+        sB[i] = d == 0 ? B : add_(sB[i], B);
+        mab[i] = s == 0 ? mul_(aj, b) : fma_(aj, b, mab[i]);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < NS; i++) {
+      const L ai = a == 0 ? x[i]->x : (a == 1 ? x[i]->y : x[i]->z);
+      e[i] = fma_(mul_(splat<L>(m.mu), ai), mab[i], e[i]);
+    }
+  }
+  const L nw = PXY ? add_(add_(w[4], w[5]), splat<L>(4.f))
+                   : add_(add_(add_(w[0], w[1]), add_(w[2], w[3])), add_(w[4], w[5]));
+  const L c = mul_(splat<L>(fmaf(-0.5f, m.nu, -m.mu / 9.f)), nw);
+#pragma unroll
+  for (int i = 0; i < NS; i++) out[i] = fma_(splat<L>(1.5f * m.nu), sB[i], add_(e[i], c));
+}
+
 template <int POT, bool PXY, bool CHIRAL, typename L>
 __device__ __forceinline__ L bond_sum(const ModelDev &m, const V3<L> &x, const V3<L> (&nb)[6], const L (&w)[6]) {
+  if (POT == POT_LL) return ll_sum<PXY>(m, x, nb, w);
+  if (POT == POT_GHRL && !CHIRAL) {
+    const V3<L> *const xs[1] = {&x};
+    L out[1];
+    ghrl_sums<PXY, 1>(m, xs, nb, w, out);
+    return out[0];
+  }
   L e = acc_bond<POT, PXY, CHIRAL, 0>(m, x, nb[0], w[0], w[0]);
   e = acc_bond<POT, PXY, CHIRAL, 1>(m, x, nb[1], w[1], e);
   e = acc_bond<POT, PXY, CHIRAL, 2>(m, x, nb[2], w[2], e);
@@ -157,6 +235,30 @@ __device__ __forceinline__ L bond_sum(const ModelDev &m, const V3<L> &x, const V
 template <int POT, bool PXY, bool CHIRAL, typename L>
 __device__ __forceinline__ void bond_sum2(const ModelDev &m, const V3<L> &x, const V3<L> &x2, const V3<L> (&nb)[6],
                                           const L (&w)[6], L &e1, L &e2) {
+  if (POT == POT_LL) {
+    L s1 = ll_acc<PXY, 0>(x, nb[0], w[0], w[0]), s2 = ll_acc<PXY, 0>(x2, nb[0], w[0], w[0]);
+    s1 = ll_acc<PXY, 1>(x, nb[1], w[1], s1);
+    s2 = ll_acc<PXY, 1>(x2, nb[1], w[1], s2);
+    s1 = ll_acc<PXY, 2>(x, nb[2], w[2], s1);
+    s2 = ll_acc<PXY, 2>(x2, nb[2], w[2], s2);
+    s1 = ll_acc<PXY, 3>(x, nb[3], w[3], s1);
+    s2 = ll_acc<PXY, 3>(x2, nb[3], w[3], s2);
+    s1 = ll_acc<PXY, 4>(x, nb[4], w[4], s1);
+    s2 = ll_acc<PXY, 4>(x2, nb[4], w[4], s2);
+    s1 = ll_acc<PXY, 5>(x, nb[5], w[5], s1);
+    s2 = ll_acc<PXY, 5>(x2, nb[5], w[5], s2);
+    e1 = mul_(splat<L>(-1.5f * m.A), s1);
+    e2 = mul_(splat<L>(-1.5f * m.A), s2);
+    return;
+  }
+  if (POT == POT_GHRL && !CHIRAL) {
+    const V3<L> *const xs[2] = {&x, &x2};
+    L out[2];
+    ghrl_sums<PXY, 2>(m, xs, nb, w, out);
+    e1 = out[0];
+    e2 = out[1];
+    return;
+  }
   e1 = acc_bond<POT, PXY, CHIRAL, 0>(m, x, nb[0], w[0], w[0]);
   e2 = acc_bond<POT, PXY, CHIRAL, 0>(m, x2, nb[0], w[0], w[0]);
   e1 = acc_bond<POT, PXY, CHIRAL, 1>(m, x, nb[1], w[1], e1);

@@ -558,12 +558,12 @@ __global__ void __launch_bounds__(NT, NT <= 256 ? 2 : 1) k_sweep_fused(ModelDev 
   }
 }
 
-// Tile configurations: rows per tile, threads per CTA (64 columns always), resident CTAs per SM, and the kernel:
-// kind 0 the fused two-colour sweep (this file), kind 1 two colour passes (sweep_pass.cuh).
+// Tile configurations: rows per tile, threads per CTA, resident CTAs per SM, the kernel (kind 0 the fused
+// two-colour sweep of this file, kind 1 two colour passes, sweep_pass.cuh) and the tile width.
 struct FusedCfg {
   int ty, nt, ctas_per_sm, kind, tx;
 };
-constexpr int kNumCfgs = 7;
+constexpr int kNumCfgs = 8;
 
 // Launch of one potential's kernels (sweep_fused_{ll,ghrl,pear}.cu): dispatch over geometry, flip, periodic x/y,
 // chirality, field and tile configuration.

@@ -36,19 +36,26 @@ void mco_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t ou
   out[3] = c3;
 }
 
+/* The engine's draw convention (mclics_b200/csrc/common.cuh): key fixed per stream, the seed in the counter
+ * (a, b, seed_lo, seed_hi + c_hi). */
+#define PHILOX_KEY0 0x694C634Du
+#define PHILOX_KEY1 0x30303242u
+static void stream_draws(uint32_t a, uint32_t b, uint64_t seed, uint32_t c_hi, uint32_t stream, uint32_t o[4]) {
+  const uint32_t ctr[4] = {a, b, (uint32_t)seed, (uint32_t)(seed >> 32) + c_hi};
+  const uint32_t key[2] = {PHILOX_KEY0 + stream, PHILOX_KEY1};
+  mco_philox4x32_10(ctr, key, o);
+}
+
 void mco_site_uniforms(uint64_t seed, uint64_t sweep, int x, int y, int z, int nx, int ny, int flip, double u[4]) {
-  uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
   uint32_t o[4];
   if (flip) {
-    uint32_t ctr[4] = {(uint32_t)x + (uint32_t)nx * ((uint32_t)y + (uint32_t)ny * (uint32_t)z), (uint32_t)sweep,
-                       (uint32_t)(sweep >> 32), 0};
-    mco_philox4x32_10(ctr, key, o);
+    stream_draws((uint32_t)x + (uint32_t)nx * ((uint32_t)y + (uint32_t)ny * (uint32_t)z), (uint32_t)sweep, seed,
+                 (uint32_t)(sweep >> 32), 0, o);
     for (int k = 0; k < 4; k++) u[k] = (double)(o[k] >> 8) * (1.0 / 16777216.0);
     return;
   }
-  uint32_t ctr[4] = {((uint32_t)x & ~2u) + (uint32_t)nx * ((uint32_t)y + (uint32_t)ny * (uint32_t)z), (uint32_t)sweep,
-                     (uint32_t)(sweep >> 32), 0};
-  mco_philox4x32_10(ctr, key, o);
+  stream_draws(((uint32_t)x & ~2u) + (uint32_t)nx * ((uint32_t)y + (uint32_t)ny * (uint32_t)z), (uint32_t)sweep, seed,
+               (uint32_t)(sweep >> 32), 0, o);
   const int h = (x >> 1) & 1;
   const uint32_t lo = o[2 * h], hi = o[2 * h + 1];
   const double s21 = 1.0 / 2097152.0;
@@ -56,6 +63,30 @@ void mco_site_uniforms(uint64_t seed, uint64_t sweep, int x, int y, int z, int n
   u[1] = (double)(((lo >> 21) | (hi << 11)) & 0x1FFFFFu) * s21;
   u[2] = (double)((hi >> 10) & 0x1FFFFFu) * s21;
   u[3] = 0;
+}
+
+/* Random initial director of a site (the engine's `ic random` on the device, Philox stream 2; the reference
+ * draws gsl_ran_dir_3d from a taus generator instead, src/ic.cpp:38-65, so parity with it is statistical): the
+ * first draw (site, attempt) whose odd-integer grid point lies inside the ball of radius 2^24, projected onto the
+ * unit sphere with one double square root and three double divisions. */
+void mco_random_director(uint64_t seed, uint32_t site, float out[3]) {
+  for (uint32_t attempt = 0; attempt < 64; attempt++) {
+    uint32_t o[4];
+    stream_draws(site, attempt, seed, 0, 2, o);
+    const int64_t ix = 2 * (int64_t)(o[0] >> 8) + 1 - 16777216, iy = 2 * (int64_t)(o[1] >> 8) + 1 - 16777216,
+                  iz = 2 * (int64_t)(o[2] >> 8) + 1 - 16777216;
+    const int64_t s = ix * ix + iy * iy + iz * iz;
+    if (s < ((int64_t)1 << 48)) {
+      const double len = sqrt((double)s);
+      out[0] = (float)((double)ix / len);
+      out[1] = (float)((double)iy / len);
+      out[2] = (float)((double)iz / len);
+      return;
+    }
+  }
+  out[0] = 0.f;
+  out[1] = 0.f;
+  out[2] = 1.f;
 }
 
 /* ------------------------------------------------------------------------------------------------ */

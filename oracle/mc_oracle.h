@@ -64,6 +64,8 @@ void mco_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t ou
  *    (x & ~2, y, z), sweep lo, sweep hi, 0); the site uses the 64-bit half h = (x >> 1) & 1 of the output, split
  *    into three 21-bit fields: u = field 2^-21; u[3] = 0. */
 void mco_site_uniforms(uint64_t seed, uint64_t sweep, int x, int y, int z, int nx, int ny, int flip, double u[4]);
+/* Random initial director of a site (Philox stream 2): see mc_oracle.c. */
+void mco_random_director(uint64_t seed, uint32_t site, float out[3]);
 
 /* Site energy of site idx with its director replaced by n (reference geometry*::site_energy). */
 float mco_site_energy(const mco_model *m, const mco_lattice *L, const float *ni, int idx, const float n[3]);

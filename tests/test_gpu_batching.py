@@ -83,7 +83,7 @@ def test_set_plan_applies_a_plan_and_keeps_the_physics():
     a, b = make(), make()
     b.set_plan(3, 8)
     p = b.plan()
-    assert (p["tile_config"], p["rows_per_tile"], p["threads_per_cta"], p["planes_per_segment"]) == (3, 32, 512, 8)
+    assert (p["tile_config"], p["rows_per_tile"], p["threads_per_cta"], p["planes_per_segment"]) == (3, 16, 256, 8)
     assert p["work_items"] > 0
     with pytest.raises(M.McLicsError) as ei:
         b.set_plan(99, 0)

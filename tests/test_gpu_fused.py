@@ -8,9 +8,10 @@ working."""
 import numpy as np
 import pytest
 
-# tile configurations (MCL_FUSED_CFG): "0", "1" = fused kernel (64 x 14, 64 x 28 tiles), "2"-"4" = colour passes
-KERNELS = {"fused14": "0", "fused28": "1", "pass": "2"}
-PASS_CFGS = ["2", "3", "4", "5", "6"]
+# tile configurations (MCL_FUSED_CFG): "0", "1" = fused kernel (64 x 14, 64 x 28 tiles), "2"-"5" = colour passes
+# (64 x 16 with the measured pass at 2 or 3 CTAs per SM, 64 x 16 at 2 CTAs per SM, 32 x 16)
+KERNELS = {"fused14": "0", "fused28": "1", "pass": "2", "pass32": "5"}
+PASS_CFGS = ["2", "3", "4", "5"]
 
 
 @pytest.fixture
@@ -52,6 +53,7 @@ SHAPES = [
     (68, 20, 33, "slab", (1, 1, 0)),
     (16, 16, 1, "slab", (1, 1, 0)),        # single plane (surface 1 only)
     (130, 34, 12, "slab", (0, 1, 0)),
+    (29, 10, 9, "bulk", (0, 0, 0)),        # odd nx along a free x: a pair task whose first site is beyond the edge
 ]
 
 
