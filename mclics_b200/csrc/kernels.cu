@@ -263,6 +263,19 @@ __global__ void k_unpack(RepDesc R, const float *__restrict__ aos, float *__rest
   }
 }
 
+// Random initial condition of one replica (random_director per site; empty sites of a point-type geometry (0, 0, 1)).
+__global__ void k_random_ic(RepDesc R, const uint8_t *__restrict__ pt, unsigned long long seed, float *__restrict__ dir) {
+  const long long N = (long long)R.nx * R.ny * R.nz;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < N; q += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(q % R.nx);
+    const long long row = q / R.nx;
+    const int y = (int)(row % R.ny), z = (int)(row / R.ny);
+    float n[3] = {0.f, 0.f, 1.f};
+    if (!pt || pt[R.site_off + q] != 0) random_director(seed, (uint32_t)q, n);
+    for (int c = 0; c < 3; c++) dir[dir_index(R, c, x, y, z)] = n[c];
+  }
+}
+
 __global__ void k_pack(RepDesc R, const float *__restrict__ dir, float *__restrict__ aos) {
   const long long N = (long long)R.nx * R.ny * R.nz;
   for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < N; q += (long long)gridDim.x * blockDim.x) {
@@ -450,6 +463,11 @@ cudaError_t launch_refresh_ghosts(const LaunchCtx &c, int max_ny_nz, int max_px_
 cudaError_t launch_unpack(const LaunchCtx &c, int replica, const RepDesc &R, const float *aos) {
   (void)replica;
   k_unpack<<<4 * 148, kThreads, 0, c.stream>>>(R, aos, c.dir);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_random_ic(const LaunchCtx &c, const RepDesc &R, unsigned long long seed) {
+  k_random_ic<<<4 * 148, kThreads, 0, c.stream>>>(R, R.geo == GEO_PT ? c.pt : nullptr, seed, c.dir);
   return cudaGetLastError();
 }
 

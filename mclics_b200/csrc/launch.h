@@ -88,5 +88,7 @@ cudaError_t launch_sweep_learned(const LaunchCtx &c, int geo, const BlockTable &
 // AoS (reference layout) <-> padded SoA for one replica.
 cudaError_t launch_unpack(const LaunchCtx &c, int replica, const RepDesc &host_desc, const float *aos);
 cudaError_t launch_pack(const LaunchCtx &c, int replica, const RepDesc &host_desc, float *aos);
+// Random initial directors of one replica (common.cuh random_director, Philox stream 2 keyed by `seed`).
+cudaError_t launch_random_ic(const LaunchCtx &c, const RepDesc &host_desc, unsigned long long seed);
 
 }  // namespace mcl

@@ -65,6 +65,7 @@ def lib():
         L.mco_ref8_stream.argtypes = [P(Model), P(Lattice), ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p,
                                       ctypes.c_int64]
         L.mco_ref8_stream.restype = ctypes.c_int64
+        L.mco_random_director.argtypes = [ctypes.c_uint64, ctypes.c_uint32, P(ctypes.c_float)]
         _lib = L
     return _lib
 
@@ -81,6 +82,16 @@ def site_uniforms(seed, sweep, x, y, z, nx, ny, flip):
     u = (ctypes.c_double * 4)()
     lib().mco_site_uniforms(seed, sweep, x, y, z, nx, ny, flip, u)
     return list(u)
+
+
+def random_directors(seed, n_sites):
+    """Random initial directors of sites 0 .. n_sites - 1 (mco_random_director), float32 (n_sites, 3)."""
+    out = np.empty((n_sites, 3), np.float32)
+    f = (ctypes.c_float * 3)()
+    for q in range(n_sites):
+        lib().mco_random_director(seed, q, f)
+        out[q] = f[:]
+    return out
 
 
 def make_model(potential="ll", A=1.0, B1=0.04, C=0.3, ghrl=(0, 0, 1, 0, 0), field_dir=(0, 0, 0), elecA=0.0,
