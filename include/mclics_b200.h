@@ -80,7 +80,7 @@ typedef struct mcl_replica {
   float T;                    /* temperature (params->T) */
   float elecE;                /* field magnitude (1 outside the electric mode) */
   float ang_var;              /* initial rotation amplitude; the reference starts every run at 0.5 */
-  unsigned long long seed;    /* Philox key of this replica */
+  unsigned long long seed;    /* seed of this replica's Philox draws (part of every draw's counter) */
 } mcl_replica;
 
 /* Observables of one replica after one sweep (FP64 reductions over FP32 site terms). */
@@ -113,6 +113,12 @@ int mcl_set_geometry(mcl_engine *e, int replica, const int *pt, const float *nor
  * zero-length directors on non-empty sites with MCL_ERR_NONFINITE and leaves the device state unchanged. */
 int mcl_upload_directors(mcl_engine *e, int replica, const float *ni);
 int mcl_download_directors(mcl_engine *e, int replica, float *ni);
+
+/* Random initial condition of one replica on the device (replaces the host loop of `ic random`,
+ * src/ic.cpp:38-65): every non-empty site gets an isotropic unit vector from Philox stream 2 keyed by `seed`
+ * (uniform point of a ball, projected onto the sphere; bit-identical to the same computation on the host), empty
+ * sites of a sphere or custom replica (0, 0, 1). Call mcl_set_geometry first for those. */
+int mcl_random_directors(mcl_engine *e, int replica, unsigned long long seed);
 
 /* Per-replica parameters; replica = -1 applies to all. T is the temperature the mode loops copy to the device
  * (src/evolve_thermal.cu:80), elecE the field magnitude the electric mode sweeps (src/evolve_electric.cu:80-82),
@@ -202,17 +208,16 @@ int mcl_local_order(mcl_engine *e, int replica, float *S);
  * CTA of one launch. A plan is a tile configuration and a number of planes per z segment. Tile configurations:
  *   0: fused sweep (both colours in one launch, ping-pong buffers), 64 x 14 sites, 256 threads per CTA;
  *   1: fused sweep, 64 x 28 sites, 512 threads;
- *   2: two in-place colour passes per sweep, 64 x 16 sites, 256 threads, 3 CTAs per SM;
- *   3: colour passes, 64 x 32 sites, 512 threads;
- *   4: colour passes, 64 x 16 sites, 256 threads, 2 CTAs per SM;
- *   5: colour passes, 64 x 16 sites, 128 threads with two pair tasks (rows r and r + 8) each, 3 CTAs per SM;
- *   6: colour passes, 32 x 16 sites, 128 threads, 5 CTAs per SM (narrow lattices waste less of a tile).
+ *   2: two in-place colour passes per sweep, 64 x 16 sites, 256 threads, 3 CTAs per SM (the measured pass 2);
+ *   3: colour passes, 64 x 16 sites, 256 threads, 3 CTAs per SM for both passes;
+ *   4: colour passes, 64 x 16 sites, 256 threads, 2 CTAs per SM (flip models: two trials per site);
+ *   5: colour passes, 32 x 16 sites, 128 threads, 5 CTAs per SM (narrow lattices waste less of a tile).
  * Every configuration gives bit-identical directors. mcl_autotune times each candidate plan for trial_sweeps
  * measured sweeps on the engine's own replicas, keeps the fastest and restores the directors, per-replica state,
  * sweep counter and series, so the run continues as if it had not been called. MCL_ERR_STATE unless the engine
  * runs the tiled sweep (bulk/slab, plain proposal, no decision recording). */
 typedef struct mcl_tuning {
-  int tile_config;        /* 0..6 as above */
+  int tile_config;        /* 0..5 as above */
   int rows_per_tile;
   int threads_per_cta;
   int planes_per_segment;
@@ -278,6 +283,11 @@ typedef struct mcl_mlp {
  * moves. Every site gets one learned trial per sweep, colour by colour (no separate n -> -n trial: the proposal is
  * symmetric under n -> -n). */
 int mcl_set_proposal(mcl_engine *e, const mcl_mlp *mlp, float kappa_max);
+/* Mixture of the learned and the plain sweep (no counterpart in the reference): with a proposal set, one learned
+ * sweep after every period - 1 plain sweeps, counted across mcl_sweeps calls from this call on; period 1 (the
+ * default) makes every sweep learned. Each sweep is an exact Metropolis(-Hastings) kernel of the same distribution,
+ * so the cycle leaves it exact. The plain sweeps adapt ang_var or not as mcl_set_adaptation says. */
+int mcl_set_proposal_mix(mcl_engine *e, int period);
 /* ang_var adaptation after each sweep (default 1, as the reference, src/evolve.cu:302-313). 0 keeps the plain
  * proposal's amplitude fixed: the fixed-amplitude yardstick of autocorrelation comparisons. */
 int mcl_set_adaptation(mcl_engine *e, int enable);

@@ -79,6 +79,7 @@ def lib():
             "mcl_set_geometry": [vp, i, vp, vp],
             "mcl_upload_directors": [vp, i, vp],
             "mcl_download_directors": [vp, i, vp],
+            "mcl_random_directors": [vp, i, ctypes.c_ulonglong],
             "mcl_set_temperature": [vp, i, f],
             "mcl_set_field": [vp, i, f],
             "mcl_set_ang_var": [vp, i, f],
@@ -101,6 +102,7 @@ def lib():
             "mcl_debug_wait_limit": [vp, ctypes.c_longlong, i],
             "mcl_profile_read": [vp, P(ctypes.c_double), P(ctypes.c_longlong), P(ctypes.c_longlong)],
             "mcl_set_proposal": [vp, vp, f],
+            "mcl_set_proposal_mix": [vp, i],
             "mcl_autotune": [vp, i, P(CTuning)],
             "mcl_measure_extras": [vp, i, P(ctypes.c_double * 3), P(CExtras)],
             "mcl_local_order": [vp, i, vp],
@@ -254,6 +256,10 @@ class Engine:
         check(lib().mcl_download_directors(self._h, r, out.ctypes.data))
         return out
 
+    def random_directors(self, r, seed):
+        """Random initial condition of replica r on the device (Philox stream 2 keyed by seed)."""
+        check(lib().mcl_random_directors(self._h, r, seed))
+
     def set_temperature(self, T, r=-1):
         check(lib().mcl_set_temperature(self._h, r, T))
 
@@ -363,6 +369,10 @@ class Engine:
             return
         p = mlp_params(params)
         check(lib().mcl_set_proposal(self._h, p.ctypes.data, kappa_max))
+
+    def set_proposal_mix(self, period):
+        """With a learned proposal set: one learned sweep after every period - 1 plain sweeps (1: all learned)."""
+        check(lib().mcl_set_proposal_mix(self._h, period))
 
     def measure_extras(self, r, director):
         """P, dtheta, divn and the radial orders of replica r's current state (director: that state's Q director)."""

@@ -489,6 +489,16 @@ int mcl_upload_directors(mcl_engine *e, int replica, const float *ni) {
   return MCL_OK;
 }
 
+int mcl_random_directors(mcl_engine *e, int replica, unsigned long long seed) {
+  int rc = check_rep(e, replica, false);
+  if (rc) return rc;
+  CK(launch_random_ic(e->ctx(), e->desc[replica], seed));
+  e->ghosts_dirty = true;
+  if ((rc = refresh_ghosts(e))) return rc;
+  CK(cudaStreamSynchronize(e->stream));
+  return kernel_errors(e);
+}
+
 int mcl_download_directors(mcl_engine *e, int replica, float *ni) {
   int rc = check_rep(e, replica, false);
   if (rc) return rc;
@@ -549,12 +559,42 @@ int mcl_get_sweep_counter(mcl_engine *e, unsigned long long *sweep) {
   return MCL_OK;
 }
 
+static int sweeps_run(mcl_engine *e, int n, int measure);
+
 int mcl_sweeps(mcl_engine *e, int n, int measure) {
   if (!e) return fail(MCL_ERR_ARG, "null engine");
   if (n < 0) return fail(MCL_ERR_ARG, "negative sweep count");
   if (e->zslab) return fail(MCL_ERR_STATE, "mcl_sweeps: a z-slab engine sweeps through the mcl_zslab_* calls");
   if (!e->geometry_set) return fail(MCL_ERR_STATE, "custom geometry: call mcl_set_geometry before sweeping");
   if (n == 0) return MCL_OK;
+  if (!e->d_mlp || e->mix_period <= 1) return sweeps_run(e, n, measure);
+  // Mixture of the learned and the plain sweep: one learned sweep after every mix_period - 1 plain ones, counted
+  // across calls. Both sweeps are exact Metropolis(-Hastings) kernels of the same distribution, so a fixed cycle
+  // of them is one too. The plain sweeps run with the learned weights set aside.
+  while (n > 0) {
+    const int until_learned = e->mix_period - 1 - e->mix_phase;
+    const bool learned = until_learned == 0;
+    const int run = learned ? 1 : std::min(n, until_learned);
+    MlpDev *weights = e->d_mlp;
+    if (!learned) e->d_mlp = nullptr;
+    const int rc = sweeps_run(e, run, measure);
+    e->d_mlp = weights;
+    if (rc) return rc;
+    e->mix_phase = (e->mix_phase + run) % e->mix_period;
+    n -= run;
+  }
+  return MCL_OK;
+}
+
+int mcl_set_proposal_mix(mcl_engine *e, int period) {
+  if (!e) return fail(MCL_ERR_ARG, "null engine");
+  if (period < 1) return fail(MCL_ERR_ARG, "mcl_set_proposal_mix: the period must be >= 1 (got %d)", period);
+  e->mix_period = period;
+  e->mix_phase = 0;
+  return MCL_OK;
+}
+
+static int sweeps_run(mcl_engine *e, int n, int measure) {
   int rc;
   if (measure && (rc = ensure_series(e, e->series_len + n))) return rc;
   const bool use_fused = e->fused && !e->record_dec && !e->d_mlp;

@@ -78,6 +78,8 @@ struct mcl_engine {
   double *d_xpart = nullptr;   // scratch of mcl_measure_extras (allocated at its first call)
   float kappa_max = 500.f;
   bool adapt = true;           // ang_var adaptation after each sweep (the reference's behaviour)
+  int mix_period = 1;          // with a learned proposal: every mix_period-th sweep learned, the others plain
+  int mix_phase = 0;           // sweeps since the last learned one (mcl_set_proposal_mix)
   bool use_graphs = false;     // fused sweeps replayed from captured CUDA graphs (one or two sweeps each)
   cudaGraphExec_t graph[2] = {nullptr, nullptr};  // [measure]: the sweeps of one replay, from buffer graph_cur
   int graph_cur[2] = {0, 0};
