@@ -1,9 +1,10 @@
-"""Ensemble parity with the reference: the same thermal scan (16^3 periodic LL, T = 1.3, 1.1, 0.9, MCT 400, MCS 1000,
-random initial condition) for the same 12 seeds, run by the reference's own CPU program (the golden fixture,
-tests/golden/ensemble_ll16.json, made by tests/golden/make_ensemble.py) and by this build's driver on the GPU. The
-two are different Markov chains (two-colour vs eight-sublattice order, Philox vs the reference's generators) with
-the same equilibrium, so for every temperature the seed means of S, varS, E and varE must agree within 3 standard
-errors (the two ensembles' errors combined)."""
+"""Ensemble parity with the reference: for each golden case (tests/golden/ensemble_<case>.json, made by
+tests/golden/make_ensemble.py from the reference's own CPU program) this build's driver runs the same input file for
+the same 16 seeds on the GPU. The two are different Markov chains (two-colour vs eight-sublattice order, Philox vs
+the reference's generators) with the same equilibrium, so at every scan point the seed means of every po.dat column
+(S, varS, E, varE, and P, dtheta, divn for pear) must agree within 3 standard errors, the two ensembles' errors
+combined. Cases: LL 16^3 thermal scan; the C1 scan itself (32^3 LL, 11 temperatures); C2's physics (GHRL
+1 : 0.5 : 1.5 slab, homeotropic W = 1.5); C5's physics (pear slab, planar anchoring, dipolar field, flip move)."""
 import json
 import os
 
@@ -14,10 +15,11 @@ from helpers import M, input_text, read_po
 
 pytestmark = pytest.mark.gpu
 
-GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ensemble_ll16.json")
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+CASES = ["ll16", "c1_scan", "ghrl_slab", "pear_field"]
 
 
-def run_ours(tmp_path, params, seed):
+def run_ours(tmp_path, params, seed, columns):
     d = os.path.join(str(tmp_path), "seed%d" % seed)
     os.makedirs(d)
     with open(os.path.join(d, "input.txt"), "w") as f:
@@ -29,26 +31,30 @@ def run_ours(tmp_path, params, seed):
     finally:
         os.chdir(cwd)
     header, rows = read_po(d)
-    return [[r[k] for k in ("T", "S", "varS", "E", "varE")] for r in rows]
+    assert header == columns
+    return [[r[k] for k in columns] for r in rows]
 
 
-def test_ensemble_matches_reference(tmp_path):
-    with open(GOLDEN) as f:
+@pytest.mark.parametrize("case", CASES)
+def test_ensemble_matches_reference(tmp_path, case):
+    with open(os.path.join(GOLDEN, "ensemble_%s.json" % case)) as f:
         g = json.load(f)
-    assert g["po_header"] == ["T", "S", "varS", "E", "varE"]
+    cols = g["po_header"]
     ref = np.array([g["rows"][str(s)] for s in g["seeds"]])
-    ours = np.array([run_ours(tmp_path, g["params"], s) for s in g["seeds"]])
+    ours = np.array([run_ours(tmp_path, g["params"], s, cols) for s in g["seeds"]])
     assert ours.shape == ref.shape
-    assert np.allclose(ours[:, :, 0], ref[:, :, 0])  # the same temperatures, in the same order
+    assert np.allclose(ours[:, :, 0], ref[:, :, 0])  # the same scan points, in the same order
     n = len(g["seeds"])
     report = []
     for t in range(ref.shape[1]):
-        for c, name in enumerate(["S", "varS", "E", "varE"], start=1):
+        for c in range(1, len(cols)):
             a, b = ref[:, t, c], ours[:, t, c]
             se = np.sqrt(a.var(ddof=1) / n + b.var(ddof=1) / n)
             z = (b.mean() - a.mean()) / se if se > 0 else 0.0
-            report.append((ref[0, t, 0], name, a.mean(), b.mean(), se, z))
+            report.append((cols[0], ref[0, t, 0], cols[c], a.mean(), b.mean(), se, z))
     for r in report:
-        print("T=%g %-4s reference %.6g  this build %.6g  se %.3g  z %+.2f" % r)
-    bad = [r for r in report if abs(r[5]) > 3.0]
-    assert not bad, "\n".join("T=%g %s ref %.6g ours %.6g se %.3g z %.2f" % r for r in report)
+        print("%s=%g %-6s reference %.6g  this build %.6g  se %.3g  z %+.2f" % r)
+    worst = max(abs(r[6]) for r in report)
+    print("%s: %d comparisons, largest |z| %.2f" % (case, len(report), worst))
+    bad = [r for r in report if abs(r[6]) > 3.0]
+    assert not bad, "\n".join("%s=%g %s ref %.6g ours %.6g se %.3g z %.2f" % r for r in bad)

@@ -197,6 +197,51 @@ def test_learned_sweep_keeps_the_equilibrium(trained):
     learned.close()
 
 
+EQUILIBRIUM_CASES = {
+    # C2's physics: GHRL 1 : 0.5 : 1.5 slab with homeotropic anchoring W = 1.5 on both plates
+    "ghrl_slab": (lambda: M.Model("ghrl", k=(1.0, 0.5, 1.5), surfaces=[("homeotropic", 1.5, 0, 0)] * 2),
+                  (12, 12, 8), 0.8),
+    # C5's physics: pear slab, planar degenerate anchoring, dipolar field along z. The plain sweep follows every
+    # rotation with an n -> -n trial; the learned proposal has none: it draws the new director with a random sign
+    # (its density is even in n), so both orientations are proposed directly.
+    "pear_field": (lambda: M.Model("pear", field_dir=(0, 0, 1), elecP=1.0, surfaces=[("fg", 1.0, 0, 0)] * 2),
+                   (12, 12, 8), 0.5),
+}
+
+
+@pytest.mark.parametrize("case", sorted(EQUILIBRIUM_CASES))
+def test_learned_sweep_keeps_the_equilibrium_of_c2_and_c5_physics(case):
+    """<E>, <S> and the polar order |sum n| / N of learned sweeps (untrained weights: any weights leave the
+    distribution exact) against the plain sweep's, 8 replicas each, within 4 combined standard errors."""
+    make_model, (nx, ny, nz), T = EQUILIBRIUM_CASES[case]
+    n_rep = 8
+
+    def run(learned, seed):
+        reps = [M.Replica(nx, ny, nz, "slab", (1, 1, 0), T=T, seed=seed + r) for r in range(n_rep)]
+        e = M.Engine(make_model(), reps, M.SCHED_CHECKER2)
+        for r in range(n_rep):
+            e.upload(r, rand_dirs(nx * ny * nz, seed + 100 * r, bias=1.5))
+        if learned:
+            e.set_proposal(perturbed_params(12))
+        e.sweeps(800)
+        e.clear_series()
+        e.sweeps(3000, measure=True)
+        out = []
+        for r in range(n_rep):
+            s = e.series(r)
+            out.append((s["energy"].mean(), s["S"].mean(),
+                        (np.linalg.norm(s["nsum"], axis=1) / s["n_valid"]).mean(), s["acceptance"].mean()))
+        e.close()
+        return np.array(out)
+
+    plain, learned = run(False, 31), run(True, 71)
+    assert learned[:, 3].mean() > 0.02  # the learned trials are accepted at all
+    for c, name in enumerate(["E", "S", "P"]):
+        a, b = plain[:, c], learned[:, c]
+        se = np.sqrt(a.var(ddof=1) / n_rep + b.var(ddof=1) / n_rep)
+        assert abs(a.mean() - b.mean()) < 4 * se + 1e-4, (case, name, a.mean(), b.mean(), se)
+
+
 LEARNED_SHAPES = [
     # (potential, nx, ny, nz, geometry, periodic)
     ("ll", 64, 16, 20, "bulk", (1, 1, 1)),
