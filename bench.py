@@ -31,6 +31,7 @@ Multi-GPU (torchrun): every rank sweeps its own independent replica of the workl
 """
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -44,6 +45,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 BYTES_PER_SITE_UPDATE = 24
+TIMED_TARGET_MS = 300.0  # the device-timed K-step region is repeated until the repeats span about this long
+MAX_REPEATS = 50
 METRIC = "site-updates/s"
 SEED = 7
 
@@ -122,15 +125,15 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(workload, tile_config):
+def ncu_traffic(workload, plan):
     """Per-launch DRAM bytes of the sweep kernel from the committed ncu summary (profiles/ncu_traffic.json), when
-    the summary was taken with the same kernel kind (colour passes: tile configurations 2-6) as this run."""
+    the summary was taken with exactly this run's plan ("tile configuration,planes per segment"); None otherwise."""
     p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if not os.path.exists(p):
         return None
     with open(p) as f:
         d = json.load(f).get(workload)
-    if not d or (int(d["plan"].split(",")[0]) >= 2) != (tile_config >= 2):
+    if not d or d["plan"] != plan:
         return None
     return d["dram_bytes_per_launch"]
 
@@ -222,32 +225,76 @@ class ClockSampler:
 
 def reference_cpu(steps, warmup, budget_s=150.0):
     """Times the reference's own CPU sweep + measurement (oracle/_ref/mclics_ref_timing) on all host cores, on the
-    256^3 GHRL slab."""
+    256^3 GHRL slab, from the GPU arm's own initial directors (the same (0,0,1) + noise state, bit for bit, passed
+    as a raw file). The requested warm-up sweeps run untimed; the timed sweeps are bounded by budget_s."""
     exe = os.path.join(ROOT, "oracle", "_ref", "mclics_ref_timing")
     if not os.path.exists(exe):
         return None, "oracle/_ref/mclics_ref_timing not built"
+    import shutil
     import tempfile
     cores = os.cpu_count() or 1
     d = tempfile.mkdtemp(prefix="mcl_ref_")
-    with open(os.path.join(d, "c2.txt"), "w") as f:
-        f.write(c2_input_text())
-    env = dict(os.environ, OMP_NUM_THREADS=str(cores))
+    try:
+        with open(os.path.join(d, "c2.txt"), "w") as f:
+            f.write(c2_input_text())
+        initial_state(256 ** 3, "z_noise", SEED).tofile(os.path.join(d, "start.f32"))
+        env = dict(os.environ, OMP_NUM_THREADS=str(cores))
 
-    def run(w, k):
-        p = subprocess.run([exe, "c2.txt", str(w), str(k), "1", "0.1", str(SEED)], cwd=d, env=env,
-                           capture_output=True, text=True, timeout=900)
-        if p.returncode != 0:
-            raise RuntimeError(p.stderr[-500:])
-        return json.loads(p.stdout.strip().splitlines()[-1])
+        def run(w, k):
+            p = subprocess.run([exe, "c2.txt", str(w), str(k), "1", "0", str(SEED), "start.f32"], cwd=d, env=env,
+                               capture_output=True, text=True, timeout=900)
+            if p.returncode != 0:
+                raise RuntimeError(p.stderr[-500:])
+            return json.loads(p.stdout.strip().splitlines()[-1])
 
-    # one probe step sizes the sample so that the whole run stays inside the budget
-    probe = run(0, 1)
-    per = max(probe["seconds"], 1e-3)
-    k = max(1, min(steps, int(budget_s / per) - warmup))
-    w = min(warmup, 1)
-    r = run(w, k)
+        # one probe sweep sizes the sample so that the whole run stays inside the budget
+        probe = run(0, 1)
+        per = max(probe["seconds"], 1e-3)
+        k = max(1, min(steps, int(budget_s / per) - warmup))
+        r = run(warmup, k)
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
     r["steps_requested"] = steps
+    r["warmup"] = warmup
     return r, None
+
+
+def reference_gpu(steps, variant):
+    """Context, not the reference arm: the reference's own GPU program (its .cu path, oracle/_ref/mclics_ref_gpu
+    built for sm_100, or mclics_ref_gpu_jit as shipped, PTX compiled by the driver) on the 256^3 GHRL slab, timed by
+    the reference's own differencing (paper/benchmark: a run with more sweeps minus a run with fewer). Measured
+    sweeps (thermalGPU's MCS loop: sweep, energy, lattice copied to the host, Q tensor and S there) and
+    thermalisation sweeps (MCT: the eight sublattice launches and the acceptance reduction only) separately. The
+    reference has no noisy initial condition, so it starts from (0, 0, 1)."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "mclics_ref_gpu" if variant == "sm_100" else "mclics_ref_gpu_jit")
+    if not os.path.exists(exe):
+        return None, "%s not built (make -C oracle REF=... refgpu)" % os.path.relpath(exe, ROOT)
+    import shutil
+    import tempfile
+
+    def run(mct, mcs):
+        d = tempfile.mkdtemp(prefix="mcl_refgpu_")
+        try:
+            text = c2_input_text().replace("evol thermal", "evol thermalGPU")
+            text = text.replace("MCT 200", "MCT %d" % mct).replace("MCS 1000", "MCS %d" % mcs)
+            with open(os.path.join(d, "input.txt"), "w") as f:
+                f.write(text)
+            t0 = time.perf_counter()
+            p = subprocess.run([exe, "input.txt"], cwd=d, capture_output=True, text=True, timeout=1200,
+                               env=dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count() or 1)))
+            t = time.perf_counter() - t0
+            if p.returncode != 0:
+                raise RuntimeError(p.stderr[-500:])
+            return t
+        finally:
+            shutil.rmtree(d, ignore_errors=True)
+
+    base = run(0, 1)
+    meas = run(0, 1 + steps)
+    therm = run(steps, 1)
+    sites = 256 ** 3
+    return {"measured_s_per_sweep": (meas - base) / steps, "thermalisation_s_per_sweep": (therm - base) / steps,
+            "sites": sites, "steps": steps, "runs_s": [base, meas, therm]}, None
 
 
 def gpu_arm(args, rank, world, local_rank):
@@ -286,7 +333,7 @@ def gpu_arm(args, rank, world, local_rank):
         tuning = eng.autotune(3)
     # every record the timed regions append (device steps, profiled sweeps, two end-to-end loops with warm-up)
     # fits the series, so no timed sweep reallocates it or captures its graph again
-    eng.reserve_series(eng.series_length() + 4 * args.steps + 256)
+    eng.reserve_series(eng.series_length() + (2 * MAX_REPEATS + 4) * args.steps + 256)
     eng.set_graphs(True)
     eng.sweeps(2, measure=True)  # captures the graph outside the timed region
     eng.synchronize()
@@ -296,17 +343,33 @@ def gpu_arm(args, rank, world, local_rank):
 
     clocks = ClockSampler(local_rank)
     clocks.start()
-    _, _, l0 = eng.profile_read()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    eng.sweeps(args.steps, measure=True)  # K steps = K sweeps, each with its measurement
-    e1.record(stream)
-    e1.synchronize()
-    clocks.stop()
-    dev_ms = e0.elapsed_time(e1)
+
+    def timed_steps():
+        """One timed region: exactly K steps (K sweeps, each with its measurement), events on the engine's stream,
+        synchronised on both sides."""
+        torch.cuda.synchronize()
+        e0.record(stream)
+        eng.sweeps(args.steps, measure=True)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    # A short K (the driver runs K = 20: ~5 ms) gives a timed region of a few ms, so the region is repeated until
+    # the repeats span about TIMED_TARGET_MS (at most MAX_REPEATS), and the median is reported.
+    _, _, l0 = eng.profile_read()
+    dev_all = [timed_steps()]
     _, _, l1 = eng.profile_read()
     launches = l1 - l0
+    repeats = torch.tensor([float(min(MAX_REPEATS, max(1, math.ceil(TIMED_TARGET_MS / max(dev_all[0], 1e-3)))))],
+                           dtype=torch.float64, device=dev)
+    if world > 1:  # every rank runs the same number of repeats
+        torch.distributed.all_reduce(repeats, op=torch.distributed.ReduceOp.MAX)
+    for _ in range(int(repeats.item()) - 1):
+        dev_all.append(timed_steps())
+    clocks.stop()
+    dev_ms = statistics.median(dev_all)
     # sweep-kernel time for the roofline: a separate run with per-sweep events (direct launches)
     eng.profile(True)
     ms0, n0, _ = eng.profile_read()
@@ -323,26 +386,29 @@ def gpu_arm(args, rank, world, local_rank):
     host_T = np.array([r["T"] for r in reps], dtype=np.float32)
     host_obs = np.zeros(len(reps), M.OBS_DTYPE)
 
-    def e2e_loop(lattice_down):
+    def e2e_loop(lattice_down, n_repeats):
         for _ in range(max(3, min(args.warmup, 10))):  # untimed: staging allocation, first launches
             eng.sweeps_io(1, host_T, host_obs)
             if lattice_down:
                 for i in range(len(reps)):
                     M.check(M.lib().mcl_download_directors(eng._h, i, host_ni[i].data_ptr()))
-        torch.cuda.synchronize()
-        if world > 1:
-            torch.distributed.barrier()
-        t0 = time.perf_counter()
-        for _ in range(args.steps):
-            eng.sweeps_io(1, host_T, host_obs)  # temperatures up, one measured sweep, its records down
-            if lattice_down:
-                for i in range(len(reps)):
-                    M.check(M.lib().mcl_download_directors(eng._h, i, host_ni[i].data_ptr()))
-        return time.perf_counter() - t0
+        times = []
+        for _ in range(n_repeats):  # each repeat times exactly K steps; the median is reported
+            torch.cuda.synchronize()
+            if world > 1:
+                torch.distributed.barrier()
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                eng.sweeps_io(1, host_T, host_obs)  # temperatures up, one measured sweep, its records down
+                if lattice_down:
+                    for i in range(len(reps)):
+                        M.check(M.lib().mcl_download_directors(eng._h, i, host_ni[i].data_ptr()))
+            times.append(time.perf_counter() - t0)
+        return statistics.median(times)
 
     clocks.start()
-    e2e_s = e2e_loop(False)
-    e2e_lat_s = e2e_loop(True)
+    e2e_s = e2e_loop(False, int(repeats.item()))
+    e2e_lat_s = e2e_loop(True, 1)
     clocks.stop()
 
     times = torch.tensor([dev_ms, e2e_s * 1e3, e2e_lat_s * 1e3], dtype=torch.float64, device=dev)
@@ -351,6 +417,7 @@ def gpu_arm(args, rank, world, local_rank):
     dev_ms_max, e2e_ms_max, e2e_lat_ms_max = float(times[0]), float(times[1]), float(times[2])
     eng.close()
     return dict(dev_ms=dev_ms_max, e2e_ms=e2e_ms_max, e2e_lat_ms=e2e_lat_ms_max, kernel_ms=kernel_ms,
+                timed_repeats=int(repeats.item()), dev_ms_all=dev_all,
                 launches=launches, sites=sites,
                 all_sites=all_sites,
                 n_rep=len(reps), clocks=clocks.summary(), S=float(rec["S"]), E=float(rec["energy"]),
@@ -469,14 +536,16 @@ def learned_compare(args):
     stream = torch.cuda.Stream()
     K = args.ess_sweeps
     arms = {}
-    for arm in ("plain", "learned"):
+    mixes = [int(k) for k in args.mix.split(",") if k.strip() and int(k) > 1]
+    for arm in ["plain", "learned"] + ["mix%d" % k for k in mixes]:
         e = engine(7)
         e.set_stream(stream.cuda_stream)
         e.sweeps(args.therm_sweeps)  # ~10 tau_E at T = 1.12 (tau_E ~ 500 sweeps for the plain proposal)
-        if arm == "plain":
-            e.set_adaptation(False)
-        else:
+        e.set_adaptation(False)  # every plain sweep at the amplitude adapted during the thermalisation
+        if arm != "plain":
             e.set_proposal(params)
+            if arm.startswith("mix"):  # one learned sweep after every k - 1 plain ones
+                e.set_proposal_mix(int(arm[3:]))
             e.sweeps(100)
         e.clear_series()
         e.synchronize()
@@ -499,13 +568,20 @@ def learned_compare(args):
                            "acceptance": float(sr["acceptance"].mean())}
         arms[arm] = res
         e.close()
-    per_T = {}
-    for T in labels:
-        p, l = arms["plain"][T], arms["learned"][T]
-        per_T[T] = {"ess_ratio_E": l["ess_per_s_E"] / p["ess_per_s_E"], "ess_ratio_S": l["ess_per_s_S"] / p["ess_per_s_S"],
-                    "z_E": (l["E"] - p["E"]) / float(np.hypot(l["E_err"], p["E_err"])),
-                    "z_S": (l["S"] - p["S"]) / float(np.hypot(l["S_err"], p["S_err"]))}
+    def ratios(arm):
+        out = {}
+        for T in labels:
+            p, l = arms["plain"][T], arms[arm][T]
+            out[T] = {"ess_ratio_E": l["ess_per_s_E"] / p["ess_per_s_E"],
+                      "ess_ratio_S": l["ess_per_s_S"] / p["ess_per_s_S"],
+                      "z_E": (l["E"] - p["E"]) / float(np.hypot(l["E_err"], p["E_err"])),
+                      "z_S": (l["S"] - p["S"]) / float(np.hypot(l["S_err"], p["S_err"]))}
+        return out
+
+    per_T = ratios("learned")
     tnis = labels[-1]  # c4: the highest temperature, T = 1.12 near T_NI
+    per_arm = {arm: ratios(arm) for arm in arms if arm != "plain"}
+    best = max(per_arm, key=lambda a: min(per_arm[a][tnis]["ess_ratio_E"], per_arm[a][tnis]["ess_ratio_S"]))
     line = {"metric": "ESS/s (tau_int of E and S), learned vs plain proposal, min over E and S at %s" % tnis,
             "value": min(per_T[tnis]["ess_ratio_E"], per_T[tnis]["ess_ratio_S"]), "unit": "ratio",
             "higher_is_better": True, "n_gpus": 1, "steps": K, "data": "synthetic", "dtype": "f32 / bf16 MLP",
@@ -514,7 +590,9 @@ def learned_compare(args):
             "training": {"samples": n_samples, "collect_s": t1 - t0, "train_s": t2 - t1, "steps": len(losses),
                          "loss_first": float(losses[:20].mean()), "loss_last": float(losses[-50:].mean()),
                          "seed": 3},
-            "per_T": per_T, "plain": arms["plain"], "learned": arms["learned"]}
+            "per_T": per_T, "per_arm": per_arm, "best_arm_at_T_NI": best,
+            "best_value": min(per_arm[best][tnis]["ess_ratio_E"], per_arm[best][tnis]["ess_ratio_S"]),
+            "arms": arms}
     print(json.dumps(line))
     return 0
 
@@ -524,7 +602,9 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
-    ap.add_argument("--impl", default="mclics_b200", choices=["mclics_b200", "reference"])
+    ap.add_argument("--impl", default="mclics_b200", choices=["mclics_b200", "reference", "reference-gpu"])
+    ap.add_argument("--reference-gpu-build", default="sm_100", choices=["sm_100", "as_shipped"],
+                    help="--impl reference-gpu: the build compiled for sm_100, or the one without -arch (PTX JIT)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--shard", action="store_true",
                     help="N > 1: split the workload's replicas across ranks (strong scaling) instead of one copy per rank")
@@ -535,6 +615,8 @@ def main():
                          "so shorter runs underestimate it)")
     ap.add_argument("--plan", default="",
                     help="tile configuration[,planes per z segment] instead of the autotuner (profiling runs)")
+    ap.add_argument("--mix", default="",
+                    help="--learned: also mixtures with one learned sweep every k sweeps, e.g. 2,4,8")
     ap.add_argument("--therm-sweeps", type=int, default=5000,
                     help="--learned: plain sweeps from the ordered start before both arms are measured")
     ap.add_argument("--train-samples", type=int, default=10_000_000)
@@ -559,6 +641,23 @@ def main():
                   parallelism=("replicas split across %d GPUs" % args.gpus if args.shard and args.gpus > 1
                                else "independent replicas x%d" % max(1, args.gpus)))
 
+    if args.impl == "reference-gpu":  # context only: the driver's reference arm is the CPU path above
+        if rank != 0:
+            return 0
+        r, why = reference_gpu(args.steps, args.reference_gpu_build)
+        if r is None:
+            print(json.dumps({"impl": "reference-gpu", "unavailable": why}))
+            return 0
+        v = r["sites"] / r["measured_s_per_sweep"]
+        print(json.dumps({"impl": "reference-gpu", "build": args.reference_gpu_build, "metric": METRIC, "value": v,
+                          "unit": "site-updates/s", "n_gpus": 1, "steps": r["steps"],
+                          "ms_per_step": 1e3 * r["measured_s_per_sweep"], "higher_is_better": True,
+                          "config": dict(config, start="(0, 0, 1): the reference has no noisy initial condition"),
+                          "thermalisation_sweeps_per_s_site_updates": r["sites"] / r["thermalisation_s_per_sweep"],
+                          "method": "wall time of thermalGPU runs with 1 + K and with 1 measured sweep (and K "
+                                    "thermalisation sweeps), differenced", "runs_s": r["runs_s"]}))
+        return 0
+
     if args.impl == "reference":
         if rank != 0:
             return 0
@@ -568,14 +667,15 @@ def main():
             return 0
         v = r["sites"] * r["steps"] / r["seconds"]
         line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "site-updates/s", "n_gpus": args.gpus,
-                "steps": r["steps"], "warmup": min(args.warmup, 1), "warmup_requested": args.warmup,
+                "steps": r["steps"], "warmup": r["warmup"], "steps_requested": r["steps_requested"],
                 "ms_per_step": 1e3 * r["seconds"] / r["steps"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic", "config": config,
                 "cpu_baseline": {"value": v, "unit": "site-updates/s", "cores": r["threads"], "kind": "reference",
-                                 "sample": "%d measured sweeps of the 256^3 lattice after %d warm-up (reference "
-                                           "EvolveN::Monte_Carlo_Step + energy_calculator + Q_tensor + eigen, "
-                                           "GSL replaced by the shim)" % (r["steps"], min(args.warmup, 1))},
+                                 "sample": "%d measured sweeps of the 256^3 lattice after %d warm-up sweeps, from the "
+                                           "GPU arm's initial directors (reference EvolveN::Monte_Carlo_Step + "
+                                           "energy_calculator + Q_tensor + eigen, GSL replaced by the shim)"
+                                           % (r["steps"], r["warmup"])},
                 "e2e": {"value": v, "unit": "site-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return 0
@@ -590,8 +690,8 @@ def main():
         if r is not None:
             cpu = {"value": r["sites"] * r["steps"] / r["seconds"], "unit": "site-updates/s", "cores": r["threads"],
                    "kind": "reference",
-                   "sample": "%d measured sweeps of the same 256^3 lattice after 1 warm-up, reference OpenMP CPU "
-                             "code (oracle/_ref, GSL shim)" % r["steps"]}
+                   "sample": "%d measured sweeps of the same 256^3 lattice (the GPU arm's initial directors) after 1 "
+                             "warm-up sweep, reference OpenMP CPU code (oracle/_ref, GSL shim)" % r["steps"]}
         else:
             cpu = {"value": None, "unavailable": why}
     if world > 1:
@@ -634,8 +734,12 @@ def main():
                                         "note": "plus the whole director field down every step, as the "
                                                 "reference's GPU loop copies it for its host-side Q tensor"},
         "gpu_launches": res["launches"],
+        "timing": {"repeats": res["timed_repeats"], "statistic": "median over repeats of the K-step region "
+                   "(device events; end to end: host clock)", "ms_per_step_each": [t / args.steps for t in
+                                                                                  res["dev_ms_all"]]},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": peak_kind, "traffic": ncu_traffic(args.workload, tu["tile_config"]),
+                     "peak_kind": peak_kind,
+                     "traffic": ncu_traffic(args.workload, "%d,%d" % (tu["tile_config"], tu["planes_per_segment"])),
                      "traffic_kind": "ncu dram read + write bytes per launch, cold L2 (profiles/ncu_traffic.json)",
                      "launches_per_sweep": launches_per_sweep,
                      "kernel_ms_per_launch": res["kernel_ms"] / launches_per_sweep,

@@ -24,7 +24,9 @@ def test_reference_arm_prints_the_contract_line():
         assert key in line, key
     assert line["metric"] == "site-updates/s" and line["unit"] == "site-updates/s" and line["higher_is_better"]
     assert line["config"]["workload"] == "ghrl_slab_256^3_k1:0.5:1.5_homeotropic_W1.5_T0.8"
-    assert line["value"] > 0 and line["steps"] == 1 and line["warmup"] == 1
+    # the contract's minimum of 3 warm-up sweeps applies to this arm too, and they all run
+    assert line["value"] > 0 and line["steps"] == 1 and line["warmup"] == 3
+    assert "initial directors" in line["cpu_baseline"]["sample"]
     cb = line["cpu_baseline"]
     assert cb["kind"] == "reference" and cb["value"] == line["value"] and cb["cores"] >= 1 and cb["sample"]
     assert line["e2e"] == {"value": line["value"], "unit": "site-updates/s", "h2d_bytes_per_step": 0,
