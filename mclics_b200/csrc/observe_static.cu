@@ -218,6 +218,29 @@ AddressRangeFn get_address_range() {
   return fn;
 }
 
+typedef CUresult (*PointerAttributeFn)(void *, CUpointer_attribute, CUdeviceptr);
+
+PointerAttributeFn get_pointer_attribute() {
+  static PointerAttributeFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuPointerGetAttribute", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PointerAttributeFn)p;
+  });
+  return fn;
+}
+
+// Whether ptr lies in memory mapped through the virtual-memory-management API (cuMemCreate + cuMemMap): such memory
+// is not usable with the legacy IPC calls, memory from cudaMalloc is.
+bool vmm_mapped(CUdeviceptr ptr) {
+  PointerAttributeFn attr = get_pointer_attribute();
+  int legacy = 1;
+  return attr && attr(&legacy, CU_POINTER_ATTRIBUTE_IS_LEGACY_CUDA_IPC_CAPABLE, ptr) == CUDA_SUCCESS && legacy == 0;
+}
+
 // The caller's buffer must be memory of the current device (or managed memory) holding 3 n_sites floats.
 int check_buffer(const float *d_ni, long long n_sites, int dev) {
   if (((uintptr_t)d_ni & 3u) != 0) return fail(MCL_ERR_ARG, "mcl_observe_device: d_ni is not 4-byte aligned");
@@ -239,11 +262,26 @@ int check_buffer(const float *d_ni, long long n_sites, int dev) {
     return fail(MCL_ERR_ARG, "mcl_observe_device: cannot determine the allocation that holds d_ni");
   const unsigned long long need = (unsigned long long)n_sites * 3ull * sizeof(float);
   const unsigned long long start = (unsigned long long)(uintptr_t)d_ni;
-  if (start < lo || start + need > (unsigned long long)lo + size)
+  if (start < lo) return fail(MCL_ERR_ARG, "mcl_observe_device: d_ni lies outside the allocation reported for it");
+  unsigned long long end = (unsigned long long)lo + size;
+  if (end < start + need && !vmm_mapped((CUdeviceptr)start))
     return fail(MCL_ERR_ARG,
                 "mcl_observe_device: d_ni must hold %llu bytes (3 floats per site) but its allocation ends %llu "
                 "bytes after it",
-                need, (unsigned long long)lo + size - start);
+                need, end - start);
+  // Pool allocators built on virtual memory management (cuMemCreate + cuMemMap, e.g. torch's expandable segments)
+  // map one buffer as several consecutive physical chunks, and the range query reports one chunk: such a buffer is
+  // accepted when consecutive mapped ranges, each starting where the previous one ends, cover it.
+  while (end < start + need) {
+    CUdeviceptr lo2 = 0;
+    size_t size2 = 0;
+    if (range(&lo2, &size2, (CUdeviceptr)end) != CUDA_SUCCESS || (unsigned long long)lo2 != end || size2 == 0)
+      return fail(MCL_ERR_ARG,
+                  "mcl_observe_device: d_ni must hold %llu bytes (3 floats per site) but the mapped memory from it "
+                  "ends %llu bytes after it",
+                  need, end - start);
+    end = (unsigned long long)lo2 + size2;
+  }
   return MCL_OK;
 }
 

@@ -142,3 +142,41 @@ def test_observe_device_rejects_bad_requests_before_launching():
     # the library still works afterwards
     rc, o = observe(model, M.Replica(8, 8, 8), small.data_ptr())
     assert rc == 0 and o["n_valid"] == 512
+
+
+VMM_CHILD = r'''
+import ctypes, sys
+import numpy as np
+import torch
+sys.path[:0] = [{tests!r}, {root!r}]
+import test_zz_no_alloc as t
+from helpers import M
+model = M.Model("ghrl", k=(1.0, 0.5, 1.5), surfaces=[("homeotropic", 1.5, 0, 0)] * 2)
+rep, ni, ref = t.engine_state(model, (256, 128, 96, "slab", (1, 1, 0)), seed=9)
+d_ni = torch.from_numpy(ni).cuda()  # 37.7 MB of directors: at least two of the allocator's 20 MiB mappings
+torch.cuda.synchronize()
+cuda = ctypes.CDLL("libcuda.so.1")
+base, size = ctypes.c_uint64(), ctypes.c_size_t()
+assert cuda.cuMemGetAddressRange_v2(ctypes.byref(base), ctypes.byref(size), ctypes.c_uint64(d_ni.data_ptr())) == 0
+chunks = "one mapping" if base.value + size.value >= d_ni.data_ptr() + ni.nbytes else "several mappings"
+rc, o = t.observe(model, rep, d_ni.data_ptr())
+assert rc == 0, M.lib().mcl_last_error()
+np.testing.assert_allclose(o["energy"], ref["energy"], rtol=1e-10, atol=1e-12)
+np.testing.assert_allclose(o["q"], ref["q"], rtol=0, atol=1e-12)
+print("ok", chunks)
+'''
+
+
+def test_observe_device_accepts_a_buffer_of_a_virtual_memory_pool():
+    """Pool allocators built on the virtual-memory-management API map a large buffer as several physical chunks (torch's
+    expandable segments: 20 MiB each). The call must accept such a buffer and measure it like any other."""
+    import os
+    import subprocess
+    import sys
+    tests = os.path.dirname(os.path.abspath(__file__))
+    code = VMM_CHILD.format(tests=tests, root=os.path.dirname(tests))
+    env = dict(os.environ, PYTORCH_CUDA_ALLOC_CONF="expandable_segments:True")
+    r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.strip().startswith("ok"), r.stdout
+    print(r.stdout.strip())
