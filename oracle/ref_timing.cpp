@@ -1,11 +1,13 @@
 // ref_timing — times the reference's own CPU sweep (compiled from the reference sources with the GSL shim) on
 // the host cores. Test/baseline infrastructure only.
 //
-//   mclics_ref_timing <input_file> <warmup> <steps> <measure 0|1> [noise seed]
+//   mclics_ref_timing <input_file> <warmup> <steps> <measure 0|1> [noise seed [directors.f32]]
 //
 // Set-up as src/main.cpp:86-107 + src/simulator.cpp:32-126 (through the reference's functions). If `noise` > 0
 // the initial directors get uniform noise of that amplitude per component and are renormalised (the C2 initial
-// state "(0,0,1) + noise"), drawn from a splitmix64 stream of `seed`, instead of reading a CSV file.
+// state "(0,0,1) + noise"), drawn from a splitmix64 stream of `seed`, instead of reading a CSV file. A raw file of
+// 3 Nt float32 (the reference layout, x fastest) replaces the initial directors of the non-empty sites: the GPU
+// arm of bench.py passes its own initial state this way, so both arms start from the same directors.
 // One step = EvolveN::Monte_Carlo_Step (src/evolve.cpp:85-221) and, with measure = 1, the measurement the
 // reference's mode loops do after each measurement sweep: energy_calculator + Q_tensor +
 // Eigen_value_evaluation (src/evolve_thermal.cpp:95-102). Prints one JSON line with the wall time of the timed
@@ -88,6 +90,18 @@ int main(int argc, char **argv) {
       double n = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
       for (int c = 0; c < 3; c++) ni[3 * q + c] = (float)(v[c] / n);
     }
+  }
+  if (argc > 7) {
+    FILE *f = fopen(argv[7], "rb");
+    std::vector<float> v(3 * Nt);
+    if (!f || fread(v.data(), sizeof(float), v.size(), f) != v.size()) {
+      fprintf(stderr, "cannot read %lld directors from %s\n", Nt, argv[7]);
+      return 2;
+    }
+    fclose(f);
+    for (long long q = 0; q < Nt; q++)
+      if (pt[q])
+        for (int c = 0; c < 3; c++) ni[3 * q + c] = v[3 * q + c];
   }
   if (strcasecmp(params.potential, "ll") * strcasecmp(params.potential, "lebwohl-lasher") == 0) {
     ev->geometry->bulk_potential = &Bulk_Energy_Lebwohl_Lasher;
