@@ -208,16 +208,15 @@ int mcl_local_order(mcl_engine *e, int replica, float *S);
  * CTA of one launch. A plan is a tile configuration and a number of planes per z segment. Tile configurations:
  *   0: fused sweep (both colours in one launch, ping-pong buffers), 64 x 14 sites, 256 threads per CTA;
  *   1: fused sweep, 64 x 28 sites, 512 threads;
- *   2: two in-place colour passes per sweep, 64 x 16 sites, 256 threads, 3 CTAs per SM (the measured pass 2);
- *   3: colour passes, 64 x 16 sites, 256 threads, 3 CTAs per SM for both passes;
- *   4: colour passes, 64 x 16 sites, 256 threads, 2 CTAs per SM (flip models: two trials per site);
- *   5: colour passes, 32 x 16 sites, 128 threads, 5 CTAs per SM (narrow lattices waste less of a tile).
+ *   2: two in-place colour passes per sweep, 64 x 16 sites, 256 threads, 3 CTAs per SM;
+ *   3: colour passes, 64 x 16 sites, 256 threads, 2 CTAs per SM (flip models: two trials per site);
+ *   4: colour passes, 32 x 16 sites, 128 threads, 5 CTAs per SM (narrow lattices waste less of a tile).
  * Every configuration gives bit-identical directors. mcl_autotune times each candidate plan for trial_sweeps
  * measured sweeps on the engine's own replicas, keeps the fastest and restores the directors, per-replica state,
  * sweep counter and series, so the run continues as if it had not been called. MCL_ERR_STATE unless the engine
  * runs the tiled sweep (bulk/slab, plain proposal, no decision recording). */
 typedef struct mcl_tuning {
-  int tile_config;        /* 0..5 as above */
+  int tile_config;        /* 0..4 as above */
   int rows_per_tile;
   int threads_per_cta;
   int planes_per_segment;

@@ -25,8 +25,8 @@ int fused_report_error(mcl_engine *e, unsigned int word);
 // Test hook: wait limit in ns (> 0 to change) and whether the first TMA load of every CTA is withheld.
 void fused_set_test_hooks(mcl_engine *e, long long timeout_ns, int skip_first_load);
 // Tile configuration: 0: fused, 64 x 14 tiles, 256 threads; 1: fused, 64 x 28, 512 threads; 2: colour passes,
-// 64 x 16, 256 threads, 3 CTAs/SM, the measured pass at 2; 3: the same, the measured pass at 3 CTAs/SM; 4: colour
-// passes, 64 x 16, 256 threads, 2 CTAs/SM; 5: colour passes, 32 x 16, 128 threads, 5 CTAs/SM.
+// 64 x 16, 256 threads, 3 CTAs/SM; 3: colour passes, 64 x 16, 256 threads, 2 CTAs/SM; 4: colour passes, 32 x 16,
+// 128 threads, 5 CTAs/SM.
 int fused_set_cfg(mcl_engine *e, int cfg);
 int fused_get_cfg(const mcl_engine *e, int *cfg, int *ty, int *seg, int *items);
 // Tile configuration and planes per z segment (seg <= 0: the heuristic's choice); rebuilds the work items.

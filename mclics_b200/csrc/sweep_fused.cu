@@ -12,12 +12,10 @@
 
 namespace mcl {
 
-// 0, 1: fused (7 slots of TY + 4 rows: one CTA per SM either way); 2-5: colour passes (4 slots of TY + 2 rows; 2 runs
-// its measured pass at 2 CTAs per SM, 3 at 3; 4 has 2 CTAs per SM throughout, for flip models; 5 has 32-wide tiles,
-// for lattices whose width is not a multiple of 64).
+// 0, 1: fused (7 slots of TY + 4 rows: one CTA per SM either way); 2-4: colour passes (4 slots of TY + 2 rows; 3 has
+// 2 CTAs per SM, for flip models; 4 has 32-wide tiles, for lattices whose width is not a multiple of 64).
 static const FusedCfg kCfgs[kNumCfgs] = {{14, 256, 1, 0, 64}, {28, 512, 1, 0, 64}, {16, 256, 3, 1, 64},
-                                         {16, 256, 3, 1, 64}, {16, 256, 2, 1, 64}, {16, 128, 5, 1, 32},
-                                         {16, 256, 3, 1, 64}, {16, 128, 5, 1, 32}};
+                                         {16, 256, 2, 1, 64}, {16, 128, 5, 1, 32}};
 
 struct FusedPlan {
   int cfg = 0, tx = 64, ty = 14, seg = 32;
@@ -112,12 +110,11 @@ static void choose_segments(const mcl_engine *e, FusedPlan &P, int sms) {
 
 static int choose_cfg(const mcl_engine *e) {
   // Colour passes (faster than the fused kernel on every measured workload): 3 CTAs per SM fit the 80 registers
-  // of the non-flip kernels, the measured pass runs at 2 (its FP64 partials); flip models (a second trial per site)
-  // need the 2-CTA variant's registers in both passes.
+  // of the non-flip kernels; flip models (a second trial per site) need the 2-CTA variant's registers.
   const char *env = getenv("MCL_FUSED_CFG");
   if (env) return std::max(0, std::min(kNumCfgs - 1, atoi(env)));
   const bool flip = e->model.flip != 0 || e->model.potential == POT_PEAR;
-  return flip ? 4 : 2;
+  return flip ? 3 : 2;
 }
 
 static int prepare_kernel(mcl_engine *e, FusedPlan *P);

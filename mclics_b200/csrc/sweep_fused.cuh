@@ -563,7 +563,7 @@ __global__ void __launch_bounds__(NT, NT <= 256 ? 2 : 1) k_sweep_fused(ModelDev 
 struct FusedCfg {
   int ty, nt, ctas_per_sm, kind, tx;
 };
-constexpr int kNumCfgs = 8;
+constexpr int kNumCfgs = 5;
 
 // Launch of one potential's kernels (sweep_fused_{ll,ghrl,pear}.cu): dispatch over geometry, flip, periodic x/y,
 // chirality, field and tile configuration.

@@ -33,7 +33,8 @@
 //    and unmeasured sweeps hold no accumulators. Every bond has exactly one colour-1 end, so
 //    E_total = sum_1 (2 bond + single) + sum_0 single; the colour-1 task adds the raw moments (sum n_a n_b, sum n)
 //    of its two updated sites and of the two colour-0 sites of the same cells in the other half-row (final since
-//    the colour-0 pass), summed in FP32 per task and plane, then in FP64; each thread turns its moments into
+//    the colour-0 pass), summed in FP32 over the thread's work item (at most 4 sites per plane of its segment),
+//    then in FP64 over threads, CTAs and the grid; each thread turns its moments into
 //    sum Q = 1.5 sum n_a n_b - 0.5 delta_ab N.
 //
 // Every wait on a TMA barrier is bounded by %globaltimer; on timeout the CTA sets the error word, waits (bounded)
@@ -137,10 +138,7 @@ __device__ __forceinline__ float2 lds_f2(const float *p) {
   return v;
 }
 
-// ACC: the per-thread partial sums of the measured pass, double (each plane's FP32 sums added in FP64) or float
-// (the work item's at most 4 x planes-per-segment site terms summed in FP32, the threads' sums then in FP64).
-template <int POT, int GEO, bool FLIP, bool PXY, bool CHIRAL, bool FIELD, int TY, int NT, int MINB, int TX, bool MEAS,
-          typename ACC = double>
+template <int POT, int GEO, bool FLIP, bool PXY, bool CHIRAL, bool FIELD, int TY, int NT, int MINB, int TX, bool MEAS>
 __global__ void __launch_bounds__(NT, MINB) k_sweep_pass(ModelDev m, FusedArgs a) {
   using W = PassWin<TY, TX>;
   using MP = TaskMap<TY, TX, NT>;
@@ -247,13 +245,15 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_pass(ModelDev m, FusedArgs a
 
   unsigned accepted = 0;
   int n_meas = 0;
-  ACC dacc[kPartials];
+  // The thread's sums over its work item (at most 4 sites per plane of its z segment) in FP32: ten FP32
+  // registers instead of ten FP64 pairs keep the measured pass at the unmeasured pass's occupancy. The threads' sums
+  // are then added in FP64 (warp shuffles, the CTA, the grid).
+  float facc[kPartials];
 #pragma unroll
-  for (int q = 0; q < kPartials; q++) dacc[q] = ACC(0);
-  // per-step sums of the measured sites (paired FP32 lanes), added to the partials at once
+  for (int q = 0; q < kPartials; q++) facc[q] = 0.f;
   auto add_step = [&](const float2 (&f)[kPartials]) {
 #pragma unroll
-    for (int q = 0; q < kPartials; q++) dacc[q] += (ACC)(f[q].x + f[q].y);
+    for (int q = 0; q < kPartials; q++) facc[q] += f[q].x + f[q].y;
   };
 
   bool ok = wait_plane(z0 - 1) && wait_plane(z0);
@@ -451,7 +451,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_pass(ModelDev m, FusedArgs a
     // raw moments -> sum of q = 1.5 v_a v_b - 0.5 delta_ab (partials 1..6: xx, xy, xz, yy, yz, zz)
     double dsum[kPartials];
 #pragma unroll
-    for (int q = 0; q < kPartials; q++) dsum[q] = (double)dacc[q];
+    for (int q = 0; q < kPartials; q++) dsum[q] = (double)facc[q];
 #pragma unroll
     for (int q = 1; q <= 6; q++) dsum[q] *= 1.5;
     dsum[1] -= 0.5 * n_meas;
@@ -475,13 +475,11 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_pass(ModelDev m, FusedArgs a
   }
 }
 
-// MINB: resident CTAs per SM the unmeasured passes are compiled for; MINB_MEAS: the same for the measured pass,
-// which holds the FP64 partial sums as well.
-template <int POT, int GEO, bool FLIP, bool PXY, bool CHIRAL, bool FIELD, int TY, int NT, int MINB, int TX,
-          int MINB_MEAS = MINB, typename ACC = double>
+// One tile configuration: the unmeasured passes and the measured one (the colour-1 pass of a measured sweep).
+template <int POT, int GEO, bool FLIP, bool PXY, bool CHIRAL, bool FIELD, int TY, int NT, int MINB, int TX>
 cudaError_t launch_pass_one(const ModelDev &m, const FusedArgs &a, const FusedLaunch &l) {
   auto k0 = k_sweep_pass<POT, GEO, FLIP, PXY, CHIRAL, FIELD, TY, NT, MINB, TX, false>;
-  auto k1 = k_sweep_pass<POT, GEO, FLIP, PXY, CHIRAL, FIELD, TY, NT, MINB_MEAS, TX, true, ACC>;
+  auto k1 = k_sweep_pass<POT, GEO, FLIP, PXY, CHIRAL, FIELD, TY, NT, MINB, TX, true>;
   if (l.prepare) {
     const cudaError_t e = cudaFuncSetAttribute(k0, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)l.smem);
     return e != cudaSuccess ? e : cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)l.smem);
@@ -493,18 +491,14 @@ cudaError_t launch_pass_one(const ModelDev &m, const FusedArgs &a, const FusedLa
   return cudaGetLastError();
 }
 
-// Colour-pass tile configurations (numbering continues the fused kernel's): 2: 64 x 16, 256 threads, 3 CTAs/SM, the
-// measured pass at 2 CTAs/SM (its FP64 partials would spill at 80 registers); 3: the same with the measured pass at
-// 3 CTAs/SM; 4: 64 x 16, 256 threads, 2 CTAs/SM (flip models, whose second trial needs the registers); 5: 32 x 16,
-// 128 threads, 5 CTAs/SM (narrow lattices waste less of a tile).
+// Colour-pass tile configurations (numbering continues the fused kernel's): 2: 64 x 16, 256 threads, 3 CTAs/SM;
+// 3: 64 x 16, 256 threads, 2 CTAs/SM (flip models, whose second trial needs the registers); 4: 32 x 16, 128 threads,
+// 5 CTAs/SM (narrow lattices waste less of a tile).
 template <int POT, int GEO, bool FLIP, bool PXY, bool CHIRAL, bool FIELD>
 cudaError_t launch_pass_cfg(const ModelDev &m, const FusedArgs &a, const FusedLaunch &l) {
-  if (l.cfg == 3) return launch_pass_one<POT, GEO, FLIP, PXY, CHIRAL, FIELD, 16, 256, 3, 64>(m, a, l);
-  if (l.cfg == 4) return launch_pass_one<POT, GEO, FLIP, PXY, CHIRAL, FIELD, 16, 256, 2, 64>(m, a, l);
-  if (l.cfg == 5) return launch_pass_one<POT, GEO, FLIP, PXY, CHIRAL, FIELD, 16, 128, 5, 32>(m, a, l);
-  if (l.cfg == 6) return launch_pass_one<POT, GEO, FLIP, PXY, CHIRAL, FIELD, 16, 256, 3, 64, 3, float>(m, a, l);
-  if (l.cfg == 7) return launch_pass_one<POT, GEO, FLIP, PXY, CHIRAL, FIELD, 16, 128, 5, 32, 5, float>(m, a, l);
-  return launch_pass_one<POT, GEO, FLIP, PXY, CHIRAL, FIELD, 16, 256, 3, 64, 2>(m, a, l);
+  if (l.cfg == 3) return launch_pass_one<POT, GEO, FLIP, PXY, CHIRAL, FIELD, 16, 256, 2, 64>(m, a, l);
+  if (l.cfg == 4) return launch_pass_one<POT, GEO, FLIP, PXY, CHIRAL, FIELD, 16, 128, 5, 32>(m, a, l);
+  return launch_pass_one<POT, GEO, FLIP, PXY, CHIRAL, FIELD, 16, 256, 3, 64>(m, a, l);
 }
 
 template <int POT, bool FLIP, bool CHIRAL, bool FIELD>

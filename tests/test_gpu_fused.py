@@ -8,10 +8,10 @@ working."""
 import numpy as np
 import pytest
 
-# tile configurations (MCL_FUSED_CFG): "0", "1" = fused kernel (64 x 14, 64 x 28 tiles), "2"-"5" = colour passes
-# (64 x 16 with the measured pass at 2 or 3 CTAs per SM, 64 x 16 at 2 CTAs per SM, 32 x 16)
-KERNELS = {"fused14": "0", "fused28": "1", "pass": "2", "pass32": "5"}
-PASS_CFGS = ["2", "3", "4", "5"]
+# tile configurations (MCL_FUSED_CFG): "0", "1" = fused kernel (64 x 14, 64 x 28 tiles), "2"-"4" = colour passes
+# (64 x 16 at 3 or 2 CTAs per SM, 32 x 16)
+KERNELS = {"fused14": "0", "fused28": "1", "pass": "2", "pass32": "4"}
+PASS_CFGS = ["2", "3", "4"]
 
 
 @pytest.fixture

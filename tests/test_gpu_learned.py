@@ -211,8 +211,9 @@ EQUILIBRIUM_CASES = {
 
 @pytest.mark.parametrize("case", sorted(EQUILIBRIUM_CASES))
 def test_learned_sweep_keeps_the_equilibrium_of_c2_and_c5_physics(case):
-    """<E>, <S> and the polar order |sum n| / N of learned sweeps (untrained weights: any weights leave the
-    distribution exact) against the plain sweep's, 8 replicas each, within 4 combined standard errors."""
+    """<E>, <S> and, for the polar model, the polar order |sum n| / N of learned sweeps (untrained weights: any
+    weights leave the distribution exact) against the plain sweep's, 8 replicas each, within 4 combined standard
+    errors."""
     make_model, (nx, ny, nz), T = EQUILIBRIUM_CASES[case]
     n_rep = 8
 
@@ -236,7 +237,13 @@ def test_learned_sweep_keeps_the_equilibrium_of_c2_and_c5_physics(case):
 
     plain, learned = run(False, 31), run(True, 71)
     assert learned[:, 3].mean() > 0.02  # the learned trials are accepted at all
-    for c, name in enumerate(["E", "S", "P"]):
+    # The polar order is an equilibrium observable of the polar pear model only. GHRL is invariant under flipping
+    # any single director, so its equilibrium has |sum n| / N ~ 0; the plain chain (small rotations, no flip trial)
+    # keeps the polar order of its start, while the learned proposal's random sign samples both orientations.
+    names = ["E", "S", "P"] if case == "pear_field" else ["E", "S"]
+    if case != "pear_field":
+        assert learned[:, 2].mean() < 0.1 < plain[:, 2].mean()
+    for c, name in enumerate(names):
         a, b = plain[:, c], learned[:, c]
         se = np.sqrt(a.var(ddof=1) / n_rep + b.var(ddof=1) / n_rep)
         assert abs(a.mean() - b.mean()) < 4 * se + 1e-4, (case, name, a.mean(), b.mean(), se)
