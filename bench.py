@@ -132,10 +132,11 @@ def ncu_traffic(workload, plan):
     if not os.path.exists(p):
         return None
     with open(p) as f:
-        d = json.load(f).get(workload)
-    if not d or d["plan"] != plan:
-        return None
-    return d["dram_bytes_per_launch"]
+        caps = json.load(f).get(workload) or []
+    for d in caps:  # one capture per plan the autotuner has been seen to pick for this workload
+        if d["plan"] == plan:
+            return d["dram_bytes_per_launch"]
+    return None
 
 
 class ClockSampler:
@@ -565,6 +566,8 @@ def learned_compare(args):
             res[key] = {"tau_E": tE, "window_E": wE, "tau_S": tS, "window_S": wS,
                            "ess_per_s_E": K / (2 * tE) / sec, "ess_per_s_S": K / (2 * tS) / sec,
                            "E": mE, "E_err": dE, "S": mS, "S_err": dS,
+                           "E_err_blocks": analysis.block_error(sr["energy"]),
+                           "S_err_blocks": analysis.block_error(sr["S"]),
                            "acceptance": float(sr["acceptance"].mean())}
         arms[arm] = res
         e.close()
@@ -575,7 +578,10 @@ def learned_compare(args):
             out[T] = {"ess_ratio_E": l["ess_per_s_E"] / p["ess_per_s_E"],
                       "ess_ratio_S": l["ess_per_s_S"] / p["ess_per_s_S"],
                       "z_E": (l["E"] - p["E"]) / float(np.hypot(l["E_err"], p["E_err"])),
-                      "z_S": (l["S"] - p["S"]) / float(np.hypot(l["S_err"], p["S_err"]))}
+                      "z_S": (l["S"] - p["S"]) / float(np.hypot(l["S_err"], p["S_err"])),
+                      # the same differences over batch-means errors (16 blocks per arm: no tau estimate)
+                      "z_E_blocks": (l["E"] - p["E"]) / float(np.hypot(l["E_err_blocks"], p["E_err_blocks"])),
+                      "z_S_blocks": (l["S"] - p["S"]) / float(np.hypot(l["S_err_blocks"], p["S_err_blocks"]))}
         return out
 
     per_T = ratios("learned")

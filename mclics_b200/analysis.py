@@ -51,3 +51,14 @@ def mean_and_error(x, c=5.0):
     x = np.asarray(x, np.float64)
     tau, _ = tau_int(x, c)
     return float(x.mean()), float(np.sqrt(x.var() * 2.0 * tau / x.size))
+
+
+def block_error(x, n_blocks=16):
+    """Standard error of the mean from the spread of n_blocks consecutive block means (batch means): a check on
+    mean_and_error that uses no autocorrelation estimate, valid once a block spans many tau_int."""
+    x = np.asarray(x, np.float64)
+    b = x.size // n_blocks
+    if b < 1 or n_blocks < 2:
+        return float("nan")
+    m = x[:b * n_blocks].reshape(n_blocks, b).mean(axis=1)
+    return float(m.std(ddof=1) / np.sqrt(n_blocks))

@@ -197,6 +197,34 @@ def test_learned_sweep_keeps_the_equilibrium(trained):
     learned.close()
 
 
+def test_learned_and_mixed_sweeps_keep_the_equilibrium_near_the_transition():
+    """LL at T = 1.12, just below the nematic-isotropic transition (T_NI = 1.1232), where the order fluctuates
+    slowly and a bias of the proposal would show first: 32 independent 20^3 replicas per arm, the network trained
+    on this lattice's own states; <E> and <S> of the learned arm and of the mixture (one learned sweep after every
+    plain one) against the plain arm's, errors from the spread between replicas (independent chains: no
+    autocorrelation estimate enters), within 4 combined standard errors."""
+    T, n_rep, nx = 1.12, 32, 20
+    plain = engine_ll(nx, T, 201, n_rep=n_rep)
+    E0, S0 = replica_means(plain, n_rep, 3000, 8000)
+    tr = engine_ll(nx, T, 401, n_rep=4, sweeps=1000)
+    p, _ = train_on(tr, 4, 300, snapshots=4, per=4096)
+    tr.close()
+    for arm, seed in (("learned", 601), ("mix2", 801)):
+        e = engine_ll(nx, T, seed, n_rep=n_rep)
+        e.set_proposal(p)
+        if arm == "mix2":
+            e.set_proposal_mix(2)
+        E1, S1 = replica_means(e, n_rep, 3000, 8000)
+        acc = np.mean([e.series(r)["acceptance"].mean() for r in range(n_rep)])
+        for name, a, b in [("E", E0, E1), ("S", S0, S1)]:
+            se = np.sqrt(a.var(ddof=1) / n_rep + b.var(ddof=1) / n_rep)
+            print("%s %s: plain %.6f  %s %.6f  se %.2g  z %+.2f  (acceptance %.3f)"
+                  % (arm, name, a.mean(), arm, b.mean(), se, (b.mean() - a.mean()) / se, acc))
+            assert abs(a.mean() - b.mean()) < 4 * se, (arm, name, a.mean(), b.mean(), se)
+        e.close()
+    plain.close()
+
+
 EQUILIBRIUM_CASES = {
     # C2's physics: GHRL 1 : 0.5 : 1.5 slab with homeotropic anchoring W = 1.5 on both plates
     "ghrl_slab": (lambda: M.Model("ghrl", k=(1.0, 0.5, 1.5), surfaces=[("homeotropic", 1.5, 0, 0)] * 2),

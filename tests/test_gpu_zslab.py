@@ -75,10 +75,12 @@ def test_slabs_reproduce_the_whole_lattice(case):
         np.testing.assert_array_equal(ser["acceptance"], ref_ser["acceptance"])
         np.testing.assert_array_equal(ser["ang_var"], ref_ser["ang_var"])
         np.testing.assert_array_equal(ser["sweep"], ref_ser["sweep"])
-        np.testing.assert_allclose(ser["energy"], ref_ser["energy"], rtol=1e-10, atol=1e-12)
-        np.testing.assert_allclose(ser["q"], ref_ser["q"], rtol=0, atol=1e-12)
-        np.testing.assert_allclose(ser["S"], ref_ser["S"], rtol=1e-10, atol=1e-12)
-        np.testing.assert_allclose(ser["nsum"], ref_ser["nsum"], rtol=1e-10, atol=1e-9)
+        # a slab's work items end at its own planes, so the per-thread FP32 sums group the site terms differently
+        # from the whole lattice's (FP64 beyond the thread): agreement to FP32 rounding of those small groups
+        np.testing.assert_allclose(ser["energy"], ref_ser["energy"], rtol=1e-7, atol=0)
+        np.testing.assert_allclose(ser["q"], ref_ser["q"], rtol=0, atol=1e-8)
+        np.testing.assert_allclose(ser["S"], ref_ser["S"], rtol=1e-7, atol=0)
+        np.testing.assert_allclose(ser["nsum"], ref_ser["nsum"], rtol=0, atol=1e-6 * (nx * ny * nz) ** 0.5)
         assert np.all(ser["n_valid"] == nx * ny * nz)
     for s in slabs:
         s.eng.close()

@@ -96,3 +96,21 @@ def test_fft_tau_int_matches_direct_sums():
         t_ref, w_ref = L.tau_int(x)
         t, w = A.tau_int(x)
         assert w == w_ref and abs(t - t_ref) < 1e-9 * max(1.0, t_ref), (phi, t, t_ref, w, w_ref)
+
+
+def test_block_error_matches_the_exact_error_of_ar1_means():
+    """Batch-means error of AR(1) series against the exact standard error of their mean,
+    sqrt(var / N * (1 + phi) / (1 - phi)), over 200 series (the estimate itself scatters by ~1/sqrt(2 (B - 1)))."""
+    from mclics_b200 import analysis as A
+    rng = np.random.default_rng(5)
+    phi, n, reps = 0.9, 32000, 200
+    e = rng.normal(size=(reps, n))
+    x = np.empty_like(e)
+    x[:, 0] = e[:, 0] / np.sqrt(1 - phi ** 2)
+    for i in range(1, n):
+        x[:, i] = phi * x[:, i - 1] + e[:, i]
+    exact = np.sqrt(1 / (1 - phi ** 2) / n * (1 + phi) / (1 - phi))
+    est = np.array([A.block_error(s, 16) for s in x])
+    assert abs(np.sqrt((est ** 2).mean()) / exact - 1) < 0.05
+    # and the spread of the 200 means agrees with both
+    assert abs(x.mean(axis=1).std(ddof=1) / exact - 1) < 0.15
