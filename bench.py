@@ -133,7 +133,7 @@ def ncu_traffic(workload, plan):
         return None
     with open(p) as f:
         caps = json.load(f).get(workload) or []
-    for d in caps:  # one capture per plan the autotuner has been seen to pick for this workload
+    for d in caps if isinstance(caps, list) else [caps]:  # one capture per plan the autotuner has been seen to pick for this workload
         if d["plan"] == plan:
             return d["dram_bytes_per_launch"]
     return None

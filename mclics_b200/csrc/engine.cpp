@@ -933,9 +933,10 @@ int mcl_autotune(mcl_engine *e, int trial_sweeps, mcl_tuning *out) {
   CKT(cudaMemcpyAsync(st.data(), e->d_state, e->n_rep * sizeof(RepState), cudaMemcpyDeviceToHost, e->stream));
   CKT(cudaMemcpyAsync(&sweep0, e->d_sweep, sizeof sweep0, cudaMemcpyDeviceToHost, e->stream));
   CKT(cudaStreamSynchronize(e->stream));
+  // the candidate plan decides whether a second buffer exists: the state always goes back into buffer 0
   auto restore = [&]() -> int {
-    e->cur = cur0;
-    CK(cudaMemcpyAsync(e->d_dir[cur0], save, (size_t)e->dir_floats * sizeof(float), cudaMemcpyDeviceToDevice,
+    e->cur = 0;
+    CK(cudaMemcpyAsync(e->d_dir[0], save, (size_t)e->dir_floats * sizeof(float), cudaMemcpyDeviceToDevice,
                        e->stream));
     CK(cudaMemcpyAsync(e->d_state, st.data(), e->n_rep * sizeof(RepState), cudaMemcpyHostToDevice, e->stream));
     CK(cudaMemcpyAsync(e->d_sweep, &sweep0, sizeof sweep0, cudaMemcpyHostToDevice, e->stream));

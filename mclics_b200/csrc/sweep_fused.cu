@@ -118,16 +118,51 @@ static int choose_cfg(const mcl_engine *e) {
 }
 
 static int prepare_kernel(mcl_engine *e, FusedPlan *P);
+static void free_plan(FusedPlan *P);
+
+// The fused plans read one director buffer and write the other; the colour passes and the learned passes update
+// one buffer in place. The second buffer (211 MB for a 256^3 lattice) therefore exists only while a fused plan is
+// selected: switching to an in-place plan brings the state into buffer 0 and frees buffer 1. The learned plan's
+// tensor maps name the buffers, so it is rebuilt at the next learned sweep.
+static int set_buffers(mcl_engine *e, FusedPlan *P) {
+  const bool two = P->C.kind == 0;
+  if (two == (e->d_dir[1] != nullptr)) return MCL_OK;
+  CKF(cudaStreamSynchronize(e->stream));
+  if (two) {
+    CKF(cudaMalloc(&e->d_dir[1], (size_t)e->dir_floats * sizeof(float)));
+    CKF(cudaMemsetAsync(e->d_dir[1], 0, (size_t)e->dir_floats * sizeof(float), e->stream));
+  } else {
+    if (e->cur == 1)
+      CKF(cudaMemcpyAsync(e->d_dir[0], e->d_dir[1], (size_t)e->dir_floats * sizeof(float), cudaMemcpyDeviceToDevice,
+                          e->stream));
+    CKF(cudaStreamSynchronize(e->stream));
+    CKF(cudaFree(e->d_dir[1]));
+    e->d_dir[1] = nullptr;
+    e->cur = 0;
+  }
+  if (P->lplan) {
+    free_plan(P->lplan);
+    delete P->lplan;
+    P->lplan = nullptr;
+  }
+  return MCL_OK;
+}
 
 static int build_items(mcl_engine *e, FusedPlan *P) {
-  if (!P->learned) P->C = kCfgs[P->cfg];
+  if (!P->learned) {
+    P->C = kCfgs[P->cfg];
+    const int rc = set_buffers(e, P);
+    if (rc) return rc;
+  }
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device);
   choose_segments(e, *P, sms);
+  // maps of buffer 0 and buffer 1 per replica (buffer 0's twice while there is one buffer: the state is in buffer 0)
   std::vector<CUtensorMap> maps(2 * e->n_rep);
   for (int r = 0; r < e->n_rep; r++)
     for (int b = 0; b < 2; b++) {
-      int rc = encode_map(&maps[2 * r + b], e->d_dir[b], e->desc[r], P->tx / 2 + 8, P->ty + (P->C.kind ? 2 : 4));
+      int rc = encode_map(&maps[2 * r + b], e->d_dir[e->d_dir[1] ? b : 0], e->desc[r], P->tx / 2 + 8,
+                          P->ty + (P->C.kind ? 2 : 4));
       if (rc) return rc;
     }
   cudaFree(P->d_tmaps);
@@ -164,8 +199,6 @@ int fused_create(mcl_engine *e) {
   FusedPlan *P = new FusedPlan();
   e->fused = P;
   P->cfg = choose_cfg(e);
-  CKF(cudaMalloc(&e->d_dir[1], (size_t)e->dir_floats * sizeof(float)));
-  CKF(cudaMemsetAsync(e->d_dir[1], 0, (size_t)e->dir_floats * sizeof(float), e->stream));
   CKF(cudaMalloc(&P->d_err, sizeof(unsigned int)));
   CKF(cudaMemset(P->d_err, 0, sizeof(unsigned int)));
   return build_items(e, P);

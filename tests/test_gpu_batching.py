@@ -38,7 +38,7 @@ def test_autotune_restores_the_state_and_keeps_the_physics():
     before = snapshot(e)
     t = e.autotune(2)
     assert t["candidates"] >= 2 and t["threads_per_cta"] in (128, 256, 512) and t["work_items"] > 0
-    assert 0 <= t["tile_config"] <= 6
+    assert 0 <= t["tile_config"] <= 4
     assert t["ms_per_sweep"] <= t["ms_default"] * (1 + 1e-9)
     after = snapshot(e)
     for a, b in zip(before[0], after[0]):
@@ -96,5 +96,29 @@ def test_set_plan_applies_a_plan_and_keeps_the_physics():
         e.sweeps(3, measure=True)
     for r in range(len(SIZES)):
         assert np.array_equal(a.download(r), b.download(r)), r
+    b.set_plan(2, 0)  # and in place again after an odd number of fused sweeps (the state sits in the second buffer)
+    for e in (a, b):
+        e.sweeps(2, measure=True)
+    for r in range(len(SIZES)):
+        assert np.array_equal(a.download(r), b.download(r)), r
     a.close()
     b.close()
+
+
+def test_second_buffer_exists_only_under_a_fused_plan():
+    """The in-place plans hold one director buffer; a fused plan adds the second and a colour-pass plan frees it."""
+    torch = pytest.importorskip("torch")
+    L = 128
+    e = M.Engine(M.Model("ll"), [M.Replica(L, L, L, T=1.0, seed=5)], M.SCHED_CHECKER2)
+    e.upload(0, rand_dirs(L ** 3, 7))
+    buffer_bytes = 12 * L ** 3  # at least the directors themselves
+    assert e.plan()["tile_config"] >= 2
+    free_one = torch.cuda.mem_get_info()[0]
+    e.set_plan(0, 0)
+    e.sweeps(1)
+    free_two = torch.cuda.mem_get_info()[0]
+    assert free_one - free_two >= buffer_bytes
+    e.set_plan(2, 0)
+    e.sweeps(1)
+    assert torch.cuda.mem_get_info()[0] - free_two >= buffer_bytes
+    e.close()

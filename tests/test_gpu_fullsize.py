@@ -51,11 +51,15 @@ def compare_one_sweep(e, om, L, ni, av, t):
     acc, av_next, dec, margin = O.sweep(om, L, ref, T, av, SEED, t, O.SCHED_CHECKER2, True)
     moved_gpu = np.any(got.reshape(-1, 3) != ni.reshape(-1, 3), axis=1)
     moved_ref = np.any(ref.reshape(-1, 3) != ni.reshape(-1, 3), axis=1)
-    mism = moved_gpu != moved_ref
+    # A rotation angle draw of exactly 1/2 (one site in 2^21: about 8 per sweep here) gives a zero rotation; both
+    # sides accept it, and the renormalisation (reciprocal square root here, square root and division in the
+    # oracle) may change the director by an ulp on one side only. A decision differs when the directors do.
+    differ = np.abs(got - ref).reshape(-1, 3).max(axis=1) > 1e-5
+    mism = (moved_gpu != moved_ref) & differ
     hard, near = explained_mismatches(mism, margin, NX, NY, NZ, L.c.periodic, TOL)
     n = NX * NY * NZ
-    print("sweep %d: %d of %d sites moved, %d decisions differ (%d next to the threshold)"
-          % (t, int(moved_ref.sum()), n, int(mism.sum()), near))
+    print("sweep %d: %d of %d sites moved, %d decisions differ (%d next to the threshold), %d zero rotations"
+          % (t, int(moved_ref.sum()), n, int(mism.sum()), near, int(((moved_gpu != moved_ref) & ~differ).sum())))
     assert not hard, "sweep %d: unexplained mismatches %s" % (t, hard[:10])
     assert near <= NEAR_PER_SITE * n
     agree = np.repeat(~mism, 3)

@@ -79,7 +79,7 @@ def test_slabs_reproduce_the_whole_lattice(case):
         # from the whole lattice's (FP64 beyond the thread): agreement to FP32 rounding of those small groups
         np.testing.assert_allclose(ser["energy"], ref_ser["energy"], rtol=1e-7, atol=0)
         np.testing.assert_allclose(ser["q"], ref_ser["q"], rtol=0, atol=1e-8)
-        np.testing.assert_allclose(ser["S"], ref_ser["S"], rtol=1e-7, atol=0)
+        np.testing.assert_allclose(ser["S"], ref_ser["S"], rtol=0, atol=1e-8)
         np.testing.assert_allclose(ser["nsum"], ref_ser["nsum"], rtol=0, atol=1e-6 * (nx * ny * nz) ** 0.5)
         assert np.all(ser["n_valid"] == nx * ny * nz)
     for s in slabs:

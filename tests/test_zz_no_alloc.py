@@ -50,6 +50,8 @@ CASES = {
                         (18, 22, 10, "slab", (0, 1, 0))),
     "ll_many_slots": (lambda: M.Model("ll", field_dir=(1, 0, 0), elecA=0.4),
                       (128, 96, 40, "bulk", (1, 1, 1))),   # 491,520 sites: 120 partial slots
+    "ghrl_slab_256_cubed": (lambda: M.Model("ghrl", k=(1.0, 0.5, 1.5), surfaces=[("homeotropic", 1.5, 0, 0)] * 2),
+                            (256, 256, 256, "slab", (1, 1, 0))),  # the bench lattice: 4096 partial slots
 }
 
 
