@@ -35,6 +35,7 @@ struct ModelDev {
   int potential;
   float A, B1, C;
   float lam, mu, nu, rho, sigma;  // GHRL
+  float ghrl_c0;                  // -mu / 9 - nu / 2 (the constant of every GHRL bond), fmaf(-0.5f, nu, -mu / 9.f)
   float fdir[3];
   float elecA, elecP;
   int flip;

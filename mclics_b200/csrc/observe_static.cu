@@ -344,6 +344,7 @@ extern "C" int mcl_observe_device(const mcl_model *model, const mcl_replica *rep
   m.nu = model->ghrl_nu;
   m.rho = model->ghrl_rho;
   m.sigma = model->ghrl_sigma;
+  m.ghrl_c0 = fmaf(-0.5f, m.nu, -m.mu / 9.f);  // IEEE division and fused multiply-add: the device's own value
   for (int k = 0; k < 3; k++) m.fdir[k] = model->field_dir[k];
   m.elecA = model->elecA;
   m.elecP = model->elecP;

@@ -209,7 +209,7 @@ __device__ __forceinline__ void ghrl_sums(const ModelDev &m, const V3<L> *const 
   }
   const L nw = PXY ? add_(add_(w[4], w[5]), splat<L>(4.f))
                    : add_(add_(add_(w[0], w[1]), add_(w[2], w[3])), add_(w[4], w[5]));
-  const L c = mul_(splat<L>(fmaf(-0.5f, m.nu, -m.mu / 9.f)), nw);
+  const L c = mul_(splat<L>(m.ghrl_c0), nw);
 #pragma unroll
   for (int i = 0; i < NS; i++) out[i] = fma_(splat<L>(1.5f * m.nu), sB[i], add_(e[i], c));
 }
