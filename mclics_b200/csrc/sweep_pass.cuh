@@ -270,6 +270,8 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_pass(ModelDev m, FusedArgs a
     }
   }
 
+  // single-site terms: none in a bulk lattice without a field; a slab's step body keeps them on every plane (a
+  // second, surface-only variant of the body pushes the 80-register kernels into spilling)
   constexpr bool kNever = GEO == GEO_BULK && !FIELD, kAlways = FIELD || GEO == GEO_SLAB;
   for (int k = z0; ok && k < z1; k++) {
     ok = wait_plane(k + 1);

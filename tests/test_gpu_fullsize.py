@@ -69,7 +69,8 @@ def compare_one_sweep(e, om, L, ni, av, t):
     assert o["n_valid"] == nv == n
     assert abs(o["energy"] - obs[0] / nv) <= 2e-6 * max(1.0, abs(obs[0] / nv))
     np.testing.assert_allclose(o["q"], obs[1:7] / nv, rtol=0, atol=2e-8)
-    np.testing.assert_allclose(o["nsum"], obs[7:10], rtol=0, atol=1e-6 * nv ** 0.5)
+    # sum n: per-thread FP32 sums of up to ~100 site terms, then FP64; ~1e-9 of the sum at this size
+    np.testing.assert_allclose(o["nsum"], obs[7:10], rtol=5e-9, atol=1e-6 * nv ** 0.5)
     s_ref, _ = O.largest_eigen(obs[1:7] / nv)
     assert abs(o["S"] - s_ref) < 5e-8
     if not mism.any():
