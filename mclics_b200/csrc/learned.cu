@@ -456,7 +456,10 @@ __device__ __forceinline__ Head mlp_head(const float (&o)[kOut], float kappa_max
 
 // 4 pi q(n) of the mixture at t = mu.n: 0.95 g + 0.05 with g = kappa cosh(kappa t) / sinh(kappa)
 // = kappa (e^{kappa (|t| - 1)} + e^{-kappa (|t| + 1)}) / (1 - e^{-2 kappa}); inv_den = 1 / (1 - e^{-2 kappa}),
-// e2k = e^{-2 kappa}. One exponential: the second term is e2k / the first.
+// e2k = e^{-2 kappa}. One exponential: the second term is e2k / the first. e2k comes from its own exponential, not
+// from 1 + expm1(-2 kappa): that sum cancels in FP32 (all of e^{-2 kappa} is lost for kappa > 8.7), which dropped the
+// second term and underestimated q by up to half for directors nearly perpendicular to mu, and so biased the chain
+// toward them wherever the network's kappa lies between a few and a few tens.
 __device__ __forceinline__ float q4pi(float t, float kappa, float inv_den, float e2k) {
   const float e1 = __expf(kappa * (fabsf(t) - 1.f));
   const float e2 = e1 > 1e-30f ? __fdividef(e2k, e1) : 0.f;
@@ -587,7 +590,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_sweep_learned(ModelDev m, const
       const float dE = __fadd_rn(e_new, -e_old);
       bool acc;
       if (St.T > 0.f) {  // u < e^{-dE/T} q(n) / q(n'), without logarithms
-        const float inv_den = -1.f / em1, e2k = 1.f + em1;
+        const float inv_den = -1.f / em1, e2k = expf(-2.f * h.kappa);
         const float q_old = q4pi(dot(h.mu, n), h.kappa, inv_den, e2k), q_new = q4pi(dot(h.mu, nn), h.kappa, inv_den, e2k);
         acc = u24(u.w) * q_new < __expf(-dE / St.T) * q_old;
       } else {
@@ -1084,7 +1087,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_learned_pass(ModelDev m, Learne
     const float dE = __fadd_rn(__fadd_rn(b_new, s_new), -__fadd_rn(b_old, s_old));
     bool acc;
     if (St.T > 0.f) {  // u < e^{-dE/T} q(n) / q(n'), without logarithms
-      const float inv_den = -1.f / em1, e2k = 1.f + em1;
+      const float inv_den = -1.f / em1, e2k = expf(-2.f * hd.kappa);
       const float q_old = q4pi(dot(hd.mu, n), hd.kappa, inv_den, e2k), q_new = q4pi(dot(hd.mu, nn), hd.kappa, inv_den, e2k);
       acc = u24(u.w) * q_new < __expf(-dE / St.T) * q_old;
     } else {
