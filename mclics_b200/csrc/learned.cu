@@ -471,14 +471,18 @@ __device__ __forceinline__ float q4pi(float t, float kappa, float inv_den, float
 __device__ __forceinline__ Vec3 sample_proposal(const Head &h, float em1, float u_mix, float u_w, float u_phi,
                                                 bool neg) {
   const bool uni = u_mix < kEps;
-  float w;
+  float w, r;
   Vec3 base;
   if (uni) {
     w = fmaf(2.f, u_w, -1.f);
+    r = sqrtf(fmaxf(0.f, 1.f - w * w));
     base = Vec3{0.f, 0.f, 1.f};
   } else {
-    w = 1.f + log1pf((1.f - u_w) * em1) / h.kappa;  // em1 = e^{-2 kappa} - 1
-    w = fminf(fmaxf(w, -1.f), 1.f);
+    // s = 1 - w = -log(u + (1 - u) e^{-2 kappa}) / kappa (em1 = e^{-2 kappa} - 1), and the tangential part from
+    // s (2 - s): near mu, 1 - w is a few ulps of 1 in FP32, and 1 - w^2 would lose its digits
+    const float sw = fminf(fmaxf(-log1pf((1.f - u_w) * em1) / h.kappa, 0.f), 2.f);
+    w = 1.f - sw;
+    r = sqrtf(sw * (2.f - sw));
     base = h.mu;
   }
   // orthonormal e1, e2 perpendicular to base: e1 = base x (x or y axis), e2 = base x e1
@@ -486,7 +490,6 @@ __device__ __forceinline__ Vec3 sample_proposal(const Head &h, float em1, float 
   const float i1 = rsqrtf(dot(e1, e1));
   e1 = Vec3{e1.x * i1, e1.y * i1, e1.z * i1};
   const Vec3 e2{base.y * e1.z - base.z * e1.y, base.z * e1.x - base.x * e1.z, base.x * e1.y - base.y * e1.x};
-  const float r = sqrtf(fmaxf(0.f, 1.f - w * w));
   float sp, cp;
   sincospif(2.f * u_phi, &sp, &cp);
   Vec3 v{fmaf(w, base.x, r * fmaf(cp, e1.x, sp * e2.x)), fmaf(w, base.y, r * fmaf(cp, e1.y, sp * e2.y)),
