@@ -235,10 +235,17 @@ void fused_plan_candidates(const mcl_engine *e, std::vector<std::pair<int, int>>
     P.C = kCfgs[cfg];
     choose_segments(e, P, sms);
     std::vector<int> segs = {P.seg, P.seg * 2, (P.seg + 1) / 2, maxz};
+    // lattices too small to give every SM a work item (C1's 32^3: 10 items) also try short segments in the colour
+    // passes, which trade two extra planes per item for more items in flight
+    long long tiles = 0;
+    for (auto &D : e->desc) tiles += (long long)((D.nx + P.tx - 1) / P.tx) * ((D.ny + P.ty - 1) / P.ty);
+    const bool few = P.C.kind == 1 && tiles * ((maxz + P.seg - 1) / P.seg) < sms;
+    if (few)
+      for (int sg : {2, 3, 4}) segs.push_back(sg);
     std::sort(segs.begin(), segs.end());
     segs.erase(std::unique(segs.begin(), segs.end()), segs.end());
     for (int sg : segs)
-      if (sg >= 6 || sg == maxz) out.push_back({cfg, std::min(sg, maxz)});
+      if (sg >= 6 || sg == maxz || (few && sg >= 2)) out.push_back({cfg, std::min(sg, maxz)});
   }
   std::sort(out.begin(), out.end());
   out.erase(std::unique(out.begin(), out.end()), out.end());

@@ -123,6 +123,33 @@ def test_colour_passes_equal_fused_bitwise(model, shape, cfg, monkeypatch):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("plan", [(2, 2), (3, 2), (4, 2), (4, 3)], ids=["2,2", "3,2", "4,2", "4,3"])
+@pytest.mark.parametrize("model", ["ll", "ghrl_slab", "pear_field"])
+@pytest.mark.parametrize("shape", [SHAPES[0], SHAPES[2], SHAPES[6]], ids=[SHAPE_IDS[0], SHAPE_IDS[2], SHAPE_IDS[6]])
+def test_short_segments_equal_fused_bitwise(plan, model, shape, monkeypatch):
+    """Colour passes with segments of 2 and 3 planes (the autotuner's candidates for lattices that give fewer work
+    items than SMs): the same directors, acceptance and ang_var as the fused kernel."""
+    nx, ny, nz, geo, per = shape
+    m = model_for(model, geo)
+    reps = [M.Replica(nx, ny, nz, geo, per, T=0.9, seed=99)]
+    monkeypatch.setenv("MCL_FUSED_CFG", "1")
+    a, sa, ava = run(m, reps, M.SCHED_CHECKER2, 5, True, [5])
+    monkeypatch.delenv("MCL_FUSED_CFG", raising=False)
+    e = M.Engine(m, reps, M.SCHED_CHECKER2)
+    e.upload(0, rand_dirs(nx * ny * nz, 5))
+    e.set_plan(*plan)
+    assert e.plan()["planes_per_segment"] == min(plan[1], nz)
+    e.set_sweep_counter(17)
+    e.sweeps(5, measure=True)
+    b, sb, avb = e.download(0), e.series(0), e.ang_var(0)
+    e.close()
+    np.testing.assert_array_equal(a[0], b)
+    assert ava[0] == avb
+    np.testing.assert_array_equal(sa[0]["acceptance"], sb["acceptance"])
+    np.testing.assert_allclose(sa[0]["energy"], sb["energy"], rtol=2e-6, atol=2e-6)
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("kernel_cfg", list(KERNELS.values()), ids=list(KERNELS), indirect=True)
 def test_fused_batch_of_uneven_replicas(kernel_cfg):
     m = M.Model("ll")
