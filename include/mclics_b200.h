@@ -211,10 +211,13 @@ int mcl_local_order(mcl_engine *e, int replica, float *S);
  *   2: two in-place colour passes per sweep, 64 x 16 sites, 256 threads, 3 CTAs per SM;
  *   3: colour passes, 64 x 16 sites, 256 threads, 2 CTAs per SM (flip models: two trials per site);
  *   4: colour passes, 32 x 16 sites, 128 threads, 5 CTAs per SM (narrow lattices waste less of a tile).
- * Every configuration gives bit-identical directors. mcl_autotune times each candidate plan for trial_sweeps
- * measured sweeps on the engine's own replicas, keeps the fastest and restores the directors, per-replica state,
- * sweep counter and series, so the run continues as if it had not been called. MCL_ERR_STATE unless the engine
- * runs the tiled sweep (bulk/slab, plain proposal, no decision recording). */
+ * The fused configurations need a second director buffer, allocated while one of them is selected and freed when a
+ * colour-pass configuration is selected again. Every configuration gives bit-identical directors. Candidate plans:
+ * per configuration the heuristic segment length, its double, its half and the whole depth; lattices that give
+ * fewer work items than SMs also 2-4 planes in the colour passes. mcl_autotune times each candidate plan for
+ * trial_sweeps measured sweeps on the engine's own replicas, keeps the fastest and restores the directors,
+ * per-replica state, sweep counter and series, so the run continues as if it had not been called. MCL_ERR_STATE
+ * unless the engine runs the tiled sweep (bulk/slab, plain proposal, no decision recording). */
 typedef struct mcl_tuning {
   int tile_config;        /* 0..4 as above */
   int rows_per_tile;
