@@ -468,19 +468,21 @@ __device__ __forceinline__ float q4pi(float t, float kappa, float inv_den, float
 
 // A draw from the mixture: u_mix < 0.05 uniform on the sphere, else the vMF about mu by Wood's method with a
 // random sign (em1 = expm1(-2 kappa)).
-__device__ __forceinline__ Vec3 sample_proposal(const Head &h, float em1, float u_mix, float u_w, float u_phi,
-                                                bool neg) {
+__device__ __forceinline__ Vec3 sample_proposal(const Head &h, float em1, float e2k, float u_mix, float u_w,
+                                                float u_phi, bool neg) {
   const bool uni = u_mix < kEps;
   float w, r;
   Vec3 base;
   if (uni) {
-    w = fmaf(2.f, u_w, -1.f);
-    r = sqrtf(fmaxf(0.f, 1.f - w * w));
+    w = fmaf(2.f, u_w, -1.f);  // exact, and so are 1 - w and 1 + w
+    r = sqrtf(fmaxf(0.f, (1.f - w) * (1.f + w)));
     base = Vec3{0.f, 0.f, 1.f};
   } else {
-    // s = 1 - w = -log(u + (1 - u) e^{-2 kappa}) / kappa (em1 = e^{-2 kappa} - 1), and the tangential part from
-    // s (2 - s): near mu, 1 - w is a few ulps of 1 in FP32, and 1 - w^2 would lose its digits
-    const float sw = fminf(fmaxf(-log1pf((1.f - u_w) * em1) / h.kappa, 0.f), 2.f);
+    // s = 1 - w = -log(u + (1 - u) e^{-2 kappa}) / kappa, the logarithm as log1p((1 - u) em1) for u near 1 and
+    // directly for small u, where e^{-2 kappa} (e2k) would vanish next to 1 in em1 = e^{-2 kappa} - 1; the
+    // tangential part from s (2 - s): near mu, 1 - w is a few ulps of 1 in FP32 and 1 - w^2 would lose its digits
+    const float lg = u_w > 0.5f ? log1pf((1.f - u_w) * em1) : logf(fmaf(1.f - u_w, e2k, u_w));
+    const float sw = fminf(fmaxf(-lg / h.kappa, 0.f), 2.f);
     w = 1.f - sw;
     r = sqrtf(sw * (2.f - sw));
     base = h.mu;
@@ -583,8 +585,8 @@ __global__ void __launch_bounds__(kThreads, 3) k_sweep_learned(ModelDev m, const
     if (valid) {
       const Head h = mlp_head(o, kappa_max);
       const U4 u = site_draws(R.seed, sweep, (uint32_t)site_linear(R, x, y, z), 1);
-      const float em1 = expm1f(-2.f * h.kappa);
-      const Vec3 nn = sample_proposal(h, em1, u24(u.x), u24(u.y), u24(u.z), (u.x & 1u) != 0u);
+      const float em1 = expm1f(-2.f * h.kappa), e2k = expf(-2.f * h.kappa);
+      const Vec3 nn = sample_proposal(h, em1, e2k, u24(u.x), u24(u.y), u24(u.z), (u.x & 1u) != 0u);
       float b_old, b_new;
       bond_sum2<POT, false, true, float>(m, n, nn, nb, w, b_old, b_new);
       const float s_old = single_energy<true>(m, n, sid, s, St.elecE), s_new = single_energy<true>(m, nn, sid, s, St.elecE);
@@ -593,7 +595,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_sweep_learned(ModelDev m, const
       const float dE = __fadd_rn(e_new, -e_old);
       bool acc;
       if (St.T > 0.f) {  // u < e^{-dE/T} q(n) / q(n'), without logarithms
-        const float inv_den = -1.f / em1, e2k = expf(-2.f * h.kappa);
+        const float inv_den = -1.f / em1;
         const float q_old = q4pi(dot(h.mu, n), h.kappa, inv_den, e2k), q_new = q4pi(dot(h.mu, nn), h.kappa, inv_den, e2k);
         acc = u24(u.w) * q_new < __expf(-dE / St.T) * q_old;
       } else {
@@ -1081,8 +1083,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_learned_pass(ModelDev m, Learne
     const Vec3 sn{0.f, 0.f, sz};
     const Head hd = mlp_head(o, a.kappa_max);
     const U4 u = site_draws(R.seed, sweep, (uint32_t)site_linear(R, x, y, k), 1);
-    const float em1 = expm1f(-2.f * hd.kappa);
-    const Vec3 nn = sample_proposal(hd, em1, u24(u.x), u24(u.y), u24(u.z), (u.x & 1u) != 0u);
+    const float em1 = expm1f(-2.f * hd.kappa), e2k = expf(-2.f * hd.kappa);
+    const Vec3 nn = sample_proposal(hd, em1, e2k, u24(u.x), u24(u.y), u24(u.z), (u.x & 1u) != 0u);
     float b_old, b_new;
     bond_sum2<POT, false, true, float>(m, n, nn, nb, w, b_old, b_new);
     const float s_old = single_energy<true>(m, n, sid, sn, St.elecE);
@@ -1090,7 +1092,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_learned_pass(ModelDev m, Learne
     const float dE = __fadd_rn(__fadd_rn(b_new, s_new), -__fadd_rn(b_old, s_old));
     bool acc;
     if (St.T > 0.f) {  // u < e^{-dE/T} q(n) / q(n'), without logarithms
-      const float inv_den = -1.f / em1, e2k = expf(-2.f * hd.kappa);
+      const float inv_den = -1.f / em1;
       const float q_old = q4pi(dot(hd.mu, n), hd.kappa, inv_den, e2k), q_new = q4pi(dot(hd.mu, nn), hd.kappa, inv_den, e2k);
       acc = u24(u.w) * q_new < __expf(-dE / St.T) * q_old;
     } else {

@@ -252,7 +252,7 @@ def test_fixed_proposal_replays_across_the_axis(kernel, monkeypatch):
         accepted += int(ok.sum())
         worst = max(worst, float(np.abs(x1[ok] - proposal[ok]).max(initial=0)))
     assert mismatched <= 3, mismatched
-    # many proposals lie close to mu, where the sampler takes the tangential part from 1 - w itself (sqrt(1 - w^2)
-    # from an FP32 w near 1 was off by up to 4e-5 here)
+    # many proposals lie close to the axis, where the sampler takes the tangential part from 1 - w itself
+    # (sqrt(1 - w^2) from an FP32 w near 1 was off by up to 4e-5 here)
     assert worst < 2e-5, worst
     assert accepted > 0.01 * N, accepted
