@@ -349,12 +349,17 @@ def gpu_arm(args, rank, world, local_rank):
 
     def timed_steps():
         """One timed region: exactly K steps (K sweeps, each with its measurement), events on the engine's stream,
-        synchronised on both sides."""
+        a barrier over the ranks and a device synchronisation on both sides."""
         torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
         e0.record(stream)
         eng.sweeps(args.steps, measure=True)
         e1.record(stream)
         e1.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
         return e0.elapsed_time(e1)
 
     # A short K (the driver runs K = 20: ~5 ms) gives a timed region of a few ms, so the region is repeated until
