@@ -456,6 +456,9 @@ def zslab_arm(args, rank, world, local_rank):
     slab.sweeps(args.steps, measure=True)
     e1.record(slab.stream)
     e1.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
     clocks.stop()
     t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
     if world > 1:
