@@ -457,8 +457,8 @@ __device__ __forceinline__ Head mlp_head(const float (&o)[kOut], float kappa_max
 // 4 pi q(n) of the mixture at t = mu.n: 0.95 g + 0.05 with g = kappa cosh(kappa t) / sinh(kappa)
 // = kappa (e^{kappa (|t| - 1)} + e^{-kappa (|t| + 1)}) / (1 - e^{-2 kappa}); inv_den = 1 / (1 - e^{-2 kappa}),
 // e2k = e^{-2 kappa}. One exponential: the second term is e2k / the first. e2k comes from its own exponential, not
-// from 1 + expm1(-2 kappa): that sum cancels in FP32 (all of e^{-2 kappa} is lost for kappa > 8.7), which dropped the
-// second term and underestimated q by up to half for directors nearly perpendicular to mu, and so biased the chain
+// from 1 + expm1(-2 kappa): that sum cancels in FP32 (all of e^{-2 kappa} is lost for kappa > 8.7), which would drop
+// the second term, make q wrong by up to a few per cent for directors nearly perpendicular to mu, and bias the chain
 // toward them wherever the network's kappa lies between a few and a few tens.
 __device__ __forceinline__ float q4pi(float t, float kappa, float inv_den, float e2k) {
   const float e1 = __expf(kappa * (fabsf(t) - 1.f));

@@ -13,7 +13,7 @@ Cases (one file tests/golden/ensemble_<case>.json each):
   pear_field  C5's physics on a 16 x 16 x 8 slab: pear (A, B1, C at the reference defaults), planar degenerate
               anchoring (fg) W = 1 on both plates, dipolar field along z (elecP = 1) at E = 0 and E = 2, the flip
               move on, T = 0.5, random start; at zero field polar domains coarsen over thousands of sweeps, hence
-              MCT 8000, MCS 4000 and 32 seeds.
+              MCT 8000, MCS 4000 and 64 seeds.
 """
 import json
 import os
@@ -46,7 +46,7 @@ CASES = {
                    ("elecX", 0), ("elecY", 0), ("elecZ", 1), ("elecP", 1.0), ("evol", "electric"), ("Ti", 0.5),
                    ("Ei", 0.0), ("Ef", 2.0), ("dE", 2.0), ("MCT", 8000), ("MCS", 4000), ("ic", "random")],
 }
-SEED_COUNT = {"pear_field": 32}  # the others: 16
+SEED_COUNT = {"pear_field": 64}  # the others: 16
 
 
 def input_text(params, seed):

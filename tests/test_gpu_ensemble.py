@@ -5,7 +5,7 @@ the reference's generators) with the same equilibrium, so at every scan point th
 (S, varS, E, varE, and P, dtheta, divn for pear) must agree within 3 standard errors, the two ensembles' errors
 combined, and the mean of z^2 over a case's comparisons must stay below 2.1. Cases: LL 16^3 thermal scan; the C1
 scan itself (32^3 LL, 11 temperatures); C2's physics (GHRL 1 : 0.5 : 1.5 slab, homeotropic W = 1.5); C5's physics
-(pear slab, planar anchoring, dipolar field, flip move; 32 seeds)."""
+(pear slab, planar anchoring, dipolar field, flip move; 64 seeds of the reference, 128 here)."""
 import json
 import os
 
@@ -18,6 +18,9 @@ pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 CASES = ["ll16", "c1_scan", "ghrl_slab", "pear_field"]
+# seeds run here per seed of the fixture: the two ensembles are independent (their standard errors add), and this
+# side is cheap, so the slow case's comparison is limited by the reference program's own seeds
+SEEDS_HERE = {"pear_field": 2}
 
 
 def run_ours(tmp_path, params, seed, columns):
@@ -42,15 +45,15 @@ def test_ensemble_matches_reference(tmp_path, case):
         g = json.load(f)
     cols = g["po_header"]
     ref = np.array([g["rows"][str(s)] for s in g["seeds"]])
-    ours = np.array([run_ours(tmp_path, g["params"], s, cols) for s in g["seeds"]])
-    assert ours.shape == ref.shape
-    assert np.allclose(ours[:, :, 0], ref[:, :, 0])  # the same scan points, in the same order
-    n = len(g["seeds"])
+    seeds = g["seeds"] + [10000 + s for s in range(len(g["seeds"]) * (SEEDS_HERE.get(case, 1) - 1))]
+    ours = np.array([run_ours(tmp_path, g["params"], s, cols) for s in seeds])
+    assert ours.shape[1:] == ref.shape[1:]
+    assert np.allclose(ours[0, :, 0], ref[0, :, 0])  # the same scan points, in the same order
     report = []
     for t in range(ref.shape[1]):
         for c in range(1, len(cols)):
             a, b = ref[:, t, c], ours[:, t, c]
-            se = np.sqrt(a.var(ddof=1) / n + b.var(ddof=1) / n)
+            se = np.sqrt(a.var(ddof=1) / len(a) + b.var(ddof=1) / len(b))
             z = (b.mean() - a.mean()) / se if se > 0 else 0.0
             report.append((cols[0], ref[0, t, 0], cols[c], a.mean(), b.mean(), se, z))
     for r in report:

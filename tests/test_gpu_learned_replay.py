@@ -123,8 +123,8 @@ def replay_colour(p, x_seen, colour):
     return out
 
 
-# kappa of a few, and kappa near 12, where e^{-2 kappa} is below FP32 resolution next to 1: the density's second
-# term must not come from 1 + expm1(-2 kappa) (an earlier build dropped it, halving q for directors perpendicular to mu)
+# kappa of a few, and kappa near 12, where e^{-2 kappa} is below FP32 resolution next to 1 (1 + expm1(-2 kappa) is
+# then 0, and a density built from it loses its second term)
 @pytest.mark.parametrize("kappa_bias", [2.5, 12.0])
 @pytest.mark.parametrize("kernel", ["passes", "gather"])
 def test_learned_sweep_replays_decision_by_decision(kernel, kappa_bias, monkeypatch):
@@ -193,7 +193,7 @@ def test_fixed_proposal_replays_across_the_axis(kernel, monkeypatch):
     """A proposal fixed at mu = z with kappa = 9, from directors close to the xy-plane, so that t = mu.n is near 0
     where the density's two exponential terms are equal and e^{-2 kappa} lies below FP32 resolution next to 1: every
     decision of a 48^3 sweep against the FP64 Hastings test, to 1e-4 in log units. An error of 1-2 % in q at t = 0
-    (what 1 + expm1(-2 kappa) gave in FP32, the build that had it) flips tens of these decisions."""
+    (what a density built from 1 + expm1(-2 kappa) has in FP32) flips several of these decisions."""
     if kernel == "gather":
         monkeypatch.setenv("MCL_LEARNED_KERNEL", "gather")
     else:
