@@ -204,12 +204,26 @@ int fused_create(mcl_engine *e) {
   return build_items(e, P);
 }
 
+// Selects a plan and rebuilds the work items, tensor maps and buffers for it; if that fails (an allocation), the
+// previous plan is rebuilt, so the engine keeps a consistent plan, and the first error is returned.
+static int apply_plan(mcl_engine *e, int cfg, int seg) {
+  FusedPlan *P = e->fused;
+  const int cfg0 = P->cfg, seg0 = P->seg_override;
+  P->cfg = cfg;
+  P->seg_override = seg;
+  const int rc = build_items(e, P);
+  if (rc == MCL_OK) return MCL_OK;
+  P->cfg = cfg0;
+  P->seg_override = seg0;
+  build_items(e, P);
+  return rc;
+}
+
 int fused_set_cfg(mcl_engine *e, int cfg) {
   if (!e->fused) return fail(MCL_ERR_STATE, "this engine does not use the fused tiled sweep");
   if (cfg < 0 || cfg >= kNumCfgs) return fail(MCL_ERR_ARG, "tile configuration %d outside 0..%d", cfg, kNumCfgs - 1);
   CKF(cudaStreamSynchronize(e->stream));
-  e->fused->cfg = cfg;
-  return build_items(e, e->fused);
+  return apply_plan(e, cfg, e->fused->seg_override);
 }
 
 int fused_set_plan(mcl_engine *e, int cfg, int seg) {
@@ -218,9 +232,7 @@ int fused_set_plan(mcl_engine *e, int cfg, int seg) {
   if (kCfgs[cfg].kind == 0 && e->zslab)
     return fail(MCL_ERR_STATE, "a z-slab engine runs the colour passes (tile configurations 2-%d)", kNumCfgs - 1);
   CKF(cudaStreamSynchronize(e->stream));
-  e->fused->cfg = cfg;
-  e->fused->seg_override = std::max(0, seg);
-  return build_items(e, e->fused);
+  return apply_plan(e, cfg, std::max(0, seg));
 }
 
 void fused_plan_candidates(const mcl_engine *e, std::vector<std::pair<int, int>> &out) {
