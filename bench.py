@@ -331,7 +331,7 @@ def gpu_arm(args, rank, world, local_rank):
         eng.set_plan(int(cfg_s), int(seg_s or 0))
         tuning = dict(eng.plan(), candidates=0)
     else:
-        tuning = eng.autotune(3)
+        tuning = eng.autotune(10)  # 10 sweeps per candidate: plans within 1 % of each other need them
     # every record the timed regions append (device steps, profiled sweeps, two end-to-end loops with warm-up)
     # fits the series, so no timed sweep reallocates it or captures its graph again
     eng.reserve_series(eng.series_length() + (2 * MAX_REPEATS + 4) * args.steps + 256)
