@@ -260,21 +260,14 @@ def reference_cpu(steps, warmup, budget_s=150.0):
     return r, None
 
 
-def reference_gpu(steps, variant):
-    """Context, not the reference arm: the reference's own GPU program (its .cu path, oracle/_ref/mclics_ref_gpu
-    built for sm_100, or mclics_ref_gpu_jit as shipped, PTX compiled by the driver) on the 256^3 GHRL slab, timed by
-    the reference's own differencing (paper/benchmark: a run with more sweeps minus a run with fewer). Measured
-    sweeps (thermalGPU's MCS loop: sweep, energy, lattice copied to the host, Q tensor and S there) and
-    thermalisation sweeps (MCT: the eight sublattice launches and the acceptance reduction only) separately. The
-    reference has no noisy initial condition, so it starts from (0, 0, 1)."""
-    exe = os.path.join(ROOT, "oracle", "_ref", "mclics_ref_gpu" if variant == "sm_100" else "mclics_ref_gpu_jit")
-    if not os.path.exists(exe):
-        return None, "%s not built (make -C oracle REF=... refgpu)" % os.path.relpath(exe, ROOT)
+def program_runs(exe, steps):
+    """The reference's differencing method on a whole program: wall time of thermalGPU runs of the 256^3 GHRL slab
+    input with 1 + K and with 1 measured sweep (and with K thermalisation sweeps), differenced per sweep."""
     import shutil
     import tempfile
 
     def run(mct, mcs):
-        d = tempfile.mkdtemp(prefix="mcl_refgpu_")
+        d = tempfile.mkdtemp(prefix="mcl_prog_")
         try:
             text = c2_input_text().replace("evol thermal", "evol thermalGPU")
             text = text.replace("MCT 200", "MCT %d" % mct).replace("MCS 1000", "MCS %d" % mcs)
@@ -295,7 +288,29 @@ def reference_gpu(steps, variant):
     therm = run(steps, 1)
     sites = 256 ** 3
     return {"measured_s_per_sweep": (meas - base) / steps, "thermalisation_s_per_sweep": (therm - base) / steps,
-            "sites": sites, "steps": steps, "runs_s": [base, meas, therm]}, None
+            "sites": sites, "steps": steps, "runs_s": [base, meas, therm]}
+
+
+def dropin(steps):
+    """Context: the compiled drop-in (the reference's own program with this library behind its *EvolveNGPU classes,
+    mclics_b200/adapter/_build/mclics_dropin) on the same input and by the same method as reference_gpu."""
+    exe = os.path.join(ROOT, "mclics_b200", "adapter", "_build", "mclics_dropin")
+    if not os.path.exists(exe):
+        return None, "mclics_b200/adapter/_build/mclics_dropin not built (make -C mclics_b200/adapter REF=...)"
+    return program_runs(exe, steps), None
+
+
+def reference_gpu(steps, variant):
+    """Context, not the reference arm: the reference's own GPU program (its .cu path, oracle/_ref/mclics_ref_gpu
+    built for sm_100, or mclics_ref_gpu_jit as shipped, PTX compiled by the driver) on the 256^3 GHRL slab, timed by
+    the reference's own differencing (paper/benchmark: a run with more sweeps minus a run with fewer). Measured
+    sweeps (thermalGPU's MCS loop: sweep, energy, lattice copied to the host, Q tensor and S there) and
+    thermalisation sweeps (MCT: the eight sublattice launches and the acceptance reduction only) separately. The
+    reference has no noisy initial condition, so it starts from (0, 0, 1)."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "mclics_ref_gpu" if variant == "sm_100" else "mclics_ref_gpu_jit")
+    if not os.path.exists(exe):
+        return None, "%s not built (make -C oracle REF=... refgpu)" % os.path.relpath(exe, ROOT)
+    return program_runs(exe, steps), None
 
 
 def gpu_arm(args, rank, world, local_rank):
@@ -616,7 +631,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
-    ap.add_argument("--impl", default="mclics_b200", choices=["mclics_b200", "reference", "reference-gpu"])
+    ap.add_argument("--impl", default="mclics_b200", choices=["mclics_b200", "reference", "reference-gpu", "dropin"])
     ap.add_argument("--reference-gpu-build", default="sm_100", choices=["sm_100", "as_shipped"],
                     help="--impl reference-gpu: the build compiled for sm_100, or the one without -arch (PTX JIT)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -654,6 +669,22 @@ def main():
     config = dict(config, step="1 sweep + measurement of every lattice", accumulators="f64 (energy, Q, sum n)",
                   parallelism=("replicas split across %d GPUs" % args.gpus if args.shard and args.gpus > 1
                                else "independent replicas x%d" % max(1, args.gpus)))
+
+    if args.impl == "dropin":  # context only: the reference's program with this library behind its GPU modes
+        if rank != 0:
+            return 0
+        r, why = dropin(args.steps)
+        if r is None:
+            print(json.dumps({"impl": "dropin", "unavailable": why}))
+            return 0
+        print(json.dumps({"impl": "dropin", "metric": METRIC, "value": r["sites"] / r["measured_s_per_sweep"],
+                          "unit": "site-updates/s", "n_gpus": 1, "steps": r["steps"],
+                          "ms_per_step": 1e3 * r["measured_s_per_sweep"], "higher_is_better": True,
+                          "config": dict(config, start="(0, 0, 1), as the reference program starts"),
+                          "thermalisation_sweeps_per_s_site_updates": r["sites"] / r["thermalisation_s_per_sweep"],
+                          "method": "wall time of thermalGPU runs with 1 + K and with 1 measured sweep (and K "
+                                    "thermalisation sweeps), differenced", "runs_s": r["runs_s"]}))
+        return 0
 
     if args.impl == "reference-gpu":  # context only: the driver's reference arm is the CPU path above
         if rank != 0:
