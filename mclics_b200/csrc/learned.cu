@@ -478,10 +478,11 @@ __device__ __forceinline__ Vec3 sample_proposal(const Head &h, float em1, float 
     r = sqrtf(fmaxf(0.f, (1.f - w) * (1.f + w)));
     base = Vec3{0.f, 0.f, 1.f};
   } else {
-    // s = 1 - w = -log(u + (1 - u) e^{-2 kappa}) / kappa, the logarithm as log1p((1 - u) em1) for u near 1 and
-    // directly for small u, where e^{-2 kappa} (e2k) would vanish next to 1 in em1 = e^{-2 kappa} - 1; the
-    // tangential part from s (2 - s): near mu, 1 - w is a few ulps of 1 in FP32 and 1 - w^2 would lose its digits
-    const float lg = u_w > 0.5f ? log1pf((1.f - u_w) * em1) : logf(fmaf(1.f - u_w, e2k, u_w));
+    // s = 1 - w = -log(1 + x) / kappa with x = (1 - u) em1 (em1 = e^{-2 kappa} - 1): as log1p(x) while 1 + x is
+    // at least 1/2, and as log(u + (1 - u) e^{-2 kappa}) below, where e^{-2 kappa} (e2k) would vanish next to 1 in em1;
+    // the tangential part from s (2 - s): near mu, 1 - w is a few ulps of 1 in FP32 and 1 - w^2 would lose its digits
+    const float x = (1.f - u_w) * em1;
+    const float lg = x >= -0.5f ? log1pf(x) : logf(fmaf(1.f - u_w, e2k, u_w));
     const float sw = fminf(fmaxf(-lg / h.kappa, 0.f), 2.f);
     w = 1.f - sw;
     r = sqrtf(sw * (2.f - sw));
