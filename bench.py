@@ -260,12 +260,15 @@ def reference_cpu(steps, warmup, budget_s=150.0):
     return r, None
 
 
-def program_runs(exe, k_meas, k_therm, repeats=2):
+def program_runs(exe, k_meas, k_therm, k0=200, repeats=2):
     """The reference's differencing method on a whole program (paper/benchmark: the fastest of the repetitions of a
-    run with more sweeps minus the fastest of a run with fewer): thermalGPU runs of the 256^3 GHRL slab input with
-    1 + k_meas and with 1 measured sweep, and with k_therm thermalisation sweeps. Every run writes ic.csv and one
-    snapshot (about 1 GB each for 256^3), so the runs go to /dev/shm where it exists: on disk their write time varies
-    by seconds between runs, more than the sweeps being measured."""
+    run with more sweeps minus the fastest of a run with fewer): thermalGPU runs of the 256^3 GHRL slab input, all
+    with at least k0 thermalisation sweeps, with 1 + k_meas and with 1 measured sweep, and with k0 + k_therm
+    thermalisation sweeps. The k0 sweeps give every run the same kind of final field: the snapshot writer
+    (src/io.cpp:59-89, a %g line and a local order parameter per site) takes seconds longer on a thermalised field
+    than on the homogeneous start, which a base run of one sweep would still be close to. Every run writes ic.csv
+    and one snapshot (about 1 GB each for 256^3), so the runs go to /dev/shm where it exists: on disk their write
+    time varies by seconds between runs, more than the sweeps being measured."""
     import shutil
     import tempfile
     where = None
@@ -292,13 +295,22 @@ def program_runs(exe, k_meas, k_therm, repeats=2):
             best = t if best is None else min(best, t)
         return best
 
-    base = run(0, 1)
-    meas = run(0, 1 + k_meas)
-    therm = run(k_therm, 1)
+    base = run(k0, 1)
+    meas = run(k0, 1 + k_meas)
+    therm = run(k0 + k_therm, 1)
     sites = 256 ** 3
     return {"measured_s_per_sweep": (meas - base) / k_meas, "thermalisation_s_per_sweep": (therm - base) / k_therm,
-            "sites": sites, "steps": k_meas, "thermalisation_sweeps": k_therm, "runs_s": [base, meas, therm],
-            "repeats": repeats, "run_dir": where or "default temporary directory"}
+            "sites": sites, "steps": k_meas, "thermalisation_sweeps": k_therm, "base_thermalisation_sweeps": k0,
+            "runs_s": [base, meas, therm], "repeats": repeats, "run_dir": where or "default temporary directory"}
+
+
+def program_method(r):
+    """The keys that describe a program_runs measurement in a context line."""
+    return {"method": "wall time of thermalGPU runs with K0 thermalisation sweeps and 1 + K or 1 measured sweeps, and "
+                      "with K0 + K2 thermalisation sweeps and 1 measured sweep, the fastest of %d each, differenced; "
+                      "run directory %s" % (r["repeats"], r["run_dir"]),
+            "base_thermalisation_sweeps": r["base_thermalisation_sweeps"],
+            "thermalisation_sweeps": r["thermalisation_sweeps"], "runs_s": r["runs_s"]}
 
 
 def dropin(steps):
@@ -307,7 +319,7 @@ def dropin(steps):
     exe = os.path.join(ROOT, "mclics_b200", "adapter", "_build", "mclics_dropin")
     if not os.path.exists(exe):
         return None, "mclics_b200/adapter/_build/mclics_dropin not built (make -C mclics_b200/adapter REF=...)"
-    return program_runs(exe, max(steps, 4000), max(steps, 4000)), None
+    return program_runs(exe, max(steps, 20000), max(steps, 20000)), None
 
 
 def reference_gpu(steps, variant):
@@ -320,7 +332,7 @@ def reference_gpu(steps, variant):
     exe = os.path.join(ROOT, "oracle", "_ref", "mclics_ref_gpu" if variant == "sm_100" else "mclics_ref_gpu_jit")
     if not os.path.exists(exe):
         return None, "%s not built (make -C oracle REF=... refgpu)" % os.path.relpath(exe, ROOT)
-    return program_runs(exe, steps, max(steps, 200)), None
+    return program_runs(exe, steps, max(steps, 1000)), None
 
 
 def gpu_arm(args, rank, world, local_rank):
@@ -692,10 +704,7 @@ def main():
                           "ms_per_step": 1e3 * r["measured_s_per_sweep"], "higher_is_better": True,
                           "config": dict(config, start="(0, 0, 1), as the reference program starts"),
                           "thermalisation_sweeps_per_s_site_updates": r["sites"] / r["thermalisation_s_per_sweep"],
-                          "method": "wall time of thermalGPU runs with 1 + K and with 1 measured sweep, and with K2 "
-                                    "thermalisation sweeps, the fastest of %d each, differenced; run directory %s"
-                                    % (r["repeats"], r["run_dir"]), "thermalisation_sweeps": r["thermalisation_sweeps"],
-                          "runs_s": r["runs_s"]}))
+                          **program_method(r)}))
         return 0
 
     if args.impl == "reference-gpu":  # context only: the driver's reference arm is the CPU path above
@@ -711,10 +720,7 @@ def main():
                           "ms_per_step": 1e3 * r["measured_s_per_sweep"], "higher_is_better": True,
                           "config": dict(config, start="(0, 0, 1): the reference has no noisy initial condition"),
                           "thermalisation_sweeps_per_s_site_updates": r["sites"] / r["thermalisation_s_per_sweep"],
-                          "method": "wall time of thermalGPU runs with 1 + K and with 1 measured sweep, and with K2 "
-                                    "thermalisation sweeps, the fastest of %d each, differenced; run directory %s"
-                                    % (r["repeats"], r["run_dir"]), "thermalisation_sweeps": r["thermalisation_sweeps"],
-                          "runs_s": r["runs_s"]}))
+                          **program_method(r)}))
         return 0
 
     if args.impl == "reference":
