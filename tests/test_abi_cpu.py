@@ -71,6 +71,25 @@ def test_create_rejects_bad_arguments_before_device():
         M.Engine(M.Model(), [M.Replica(8, 8, 8, geometry="slab")])  # slab without anchoring
 
 
+@pytest.mark.parametrize("sizes,text", [
+    ((0, 8, 8), "grid sizes must be >= 1"),
+    ((8, 8, 0), "grid sizes must be >= 1"),
+    ((-2, 8, 8), "grid sizes must be >= 1"),
+    ((4096, 4096, 4096), "more than 2^32 sites"),   # the Philox site counter is 32 bits wide
+    ((65536, 65536, 2), "more than 2^32 sites"),
+], ids=["empty_x", "empty_z", "negative", "cube_4096", "flat_65536"])
+def test_create_rejects_empty_and_oversized_lattices(sizes, text):
+    with pytest.raises(M.McLicsError) as ei:
+        M.Engine(M.Model(), [M.Replica(*sizes)])
+    assert ei.value.code == 1 and text in str(ei.value)
+
+
+def test_create_rejects_an_empty_batch():
+    with pytest.raises(M.McLicsError) as ei:
+        M.Engine(M.Model(), [])
+    assert ei.value.code == 1 and "no replicas" in str(ei.value)
+
+
 ERRORS = [
     ("odd_periodic", base(Nx=5), "requires an even number of sites"),
     ("wrong_dT", base(Ti=0.5, Tf=1.0, dT=-0.1), "does not lead from Ti"),
