@@ -25,7 +25,8 @@ reference's thermalGPU loop. Metric: site updates per second (whole job, all GPU
   cpu_baseline  the reference's own OpenMP CPU sweep + measurement (oracle/_ref/mclics_ref_timing, built from the
              reference sources) on all host cores, on a bounded sample of the same lattice.
 
---impl reference times that reference CPU path alone (rank 0) and prints its line with "impl": "reference".
+--impl reference times that reference CPU path alone (rank 0) and prints its line with "impl": "reference"; with
+--workload cN it times that workload's replicas (one after another, from the GPU arm's initial directors).
 Multi-GPU (torchrun): every rank sweeps its own independent replica of the workload (no data-path collective;
 "scaling": "weak"); value = all ranks' site updates / the slowest rank's device time.
 """
@@ -224,40 +225,78 @@ class ClockSampler:
                 "region": "device-timed and end-to-end-timed steps"}
 
 
-def reference_cpu(steps, warmup, budget_s=150.0):
+def reference_input_text(name, rep):
+    """The reference's input file for one replica of a workload: the lattice, physics, temperature and field of the
+    GPU arm's replica (the timing harness runs at T = Ti and, in the electric mode, at the field Ei)."""
+    if name == "c2":
+        return c2_input_text()
+    lines = ["Nx %d" % rep["nx"], "Ny %d" % rep["ny"], "Nz %d" % rep["nz"], "geometry %s" % rep["geometry"],
+             "xbound periodic", "ybound periodic", "seed %d" % rep["seed"], "ic random", "MCT 0", "MCS 1"]
+    if rep["geometry"] == "bulk":
+        lines.append("zbound periodic")
+    if name in ("c1", "c3", "c4"):
+        lines += ["potential ll", "evol thermal", "Ti %r" % rep["T"], "Tf %r" % rep["T"], "dT -0.1"]
+    elif name == "c5":
+        lines += ["potential pear", "A 1.0", "B1 0.04", "C 0.3", "anchoring_type 0 fg", "W 0 1.0",
+                  "anchoring_type 1 fg", "W 1 1.0", "elecX 0", "elecY 0", "elecZ 1", "elecP 1.0", "evol electric",
+                  "Ti %r" % rep["T"], "Ei %r" % rep["elecE"], "Ef %r" % rep["elecE"], "dE 0.1"]
+    else:
+        raise SystemExit("no reference input for workload " + name)
+    return "\n".join(lines) + "\n"
+
+
+def reference_cpu(steps, warmup, budget_s=150.0, name="c2"):
     """Times the reference's own CPU sweep + measurement (oracle/_ref/mclics_ref_timing) on all host cores, on the
-    256^3 GHRL slab, from the GPU arm's own initial directors (the same (0,0,1) + noise state, bit for bit, passed
-    as a raw file). The requested warm-up sweeps run untimed; the timed sweeps are bounded by budget_s."""
+    replicas of a workload, each from the GPU arm's own initial directors (passed as a raw file, bit for bit). One
+    step = one measured sweep of every timed replica, the replicas one after another. The requested warm-up sweeps
+    run untimed; the timed sweeps are bounded by budget_s: a probe sweep of the largest replica sizes the sample, and
+    when one step of all replicas would not fit the budget with its warm-up, every m-th replica is timed."""
     exe = os.path.join(ROOT, "oracle", "_ref", "mclics_ref_timing")
     if not os.path.exists(exe):
         return None, "oracle/_ref/mclics_ref_timing not built"
     import shutil
     import tempfile
+    _, reps, _, ic = workload(name)
+    sizes = [r["nx"] * r["ny"] * r["nz"] for r in reps]
     cores = os.cpu_count() or 1
     d = tempfile.mkdtemp(prefix="mcl_ref_")
     try:
-        with open(os.path.join(d, "c2.txt"), "w") as f:
-            f.write(c2_input_text())
-        initial_state(256 ** 3, "z_noise", SEED).tofile(os.path.join(d, "start.f32"))
         env = dict(os.environ, OMP_NUM_THREADS=str(cores))
 
-        def run(w, k):
-            p = subprocess.run([exe, "c2.txt", str(w), str(k), "1", "0", str(SEED), "start.f32"], cwd=d, env=env,
+        def run(i, w, k):
+            with open(os.path.join(d, "input.txt"), "w") as f:
+                f.write(reference_input_text(name, reps[i]))
+            initial_state(sizes[i], ic, SEED + 97 * i).tofile(os.path.join(d, "start.f32"))
+            p = subprocess.run([exe, "input.txt", str(w), str(k), "1", "0", str(SEED), "start.f32"], cwd=d, env=env,
                                capture_output=True, text=True, timeout=900)
             if p.returncode != 0:
                 raise RuntimeError(p.stderr[-500:])
             return json.loads(p.stdout.strip().splitlines()[-1])
 
-        # one probe sweep sizes the sample so that the whole run stays inside the budget
-        probe = run(0, 1)
-        per = max(probe["seconds"], 1e-3)
-        k = max(1, min(steps, int(budget_s / per) - warmup))
-        r = run(warmup, k)
+        big = max(range(len(reps)), key=lambda i: sizes[i])
+        per_site = max(run(big, 0, 1)["seconds"], 1e-4) / sizes[big]
+        m = max(1, math.ceil(per_site * sum(sizes) * (warmup + 1) / budget_s))
+        chosen = list(range(0, len(reps), m))
+        per_step = per_site * sum(sizes[i] for i in chosen)
+        k = max(1, min(steps, int(budget_s / per_step) - warmup))
+        runs = [run(i, warmup, k) for i in chosen]
     finally:
         shutil.rmtree(d, ignore_errors=True)
-    r["steps_requested"] = steps
-    r["warmup"] = warmup
+    r = {"steps": k, "seconds": sum(x["seconds"] for x in runs), "threads": runs[0]["threads"],
+         "sites": sum(sizes[i] for i in chosen), "replicas_timed": len(chosen), "replicas": len(reps),
+         "replica_stride": m, "steps_requested": steps, "warmup": warmup}
     return r, None
+
+
+def reference_sample(r, name):
+    """The sample a reference_cpu result covers, in words."""
+    which = ("the 256^3 lattice" if name == "c2" else
+             "all %d replicas" % r["replicas"] if r["replicas_timed"] == r["replicas"] and r["replicas"] > 1 else
+             "the lattice" if r["replicas"] == 1 else
+             "%d of the %d replicas (every %d-th)" % (r["replicas_timed"], r["replicas"], r["replica_stride"]))
+    return ("%d measured sweeps of %s after %d warm-up sweeps, from the GPU arm's initial directors (reference "
+            "EvolveN::Monte_Carlo_Step + energy_calculator + Q_tensor + eigen, GSL replaced by the shim)"
+            % (r["steps"], which, r["warmup"]))
 
 
 def program_runs(exe, k_meas, k_therm, k0=200, repeats=2):
@@ -687,7 +726,8 @@ def main():
         return learned_compare(args)
     if args.zslab and args.impl != "reference":
         return zslab_main(args, rank, world, local_rank)
-    _, _, config, _ = workload(args.workload) if args.impl != "reference" else workload("c2")
+    # the reference arm runs every workload; the whole-program arms (dropin, reference-gpu) run C2's input only
+    _, _, config, _ = workload(args.workload if args.impl in ("mclics_b200", "reference") else "c2")
     config = dict(config, step="1 sweep + measurement of every lattice", accumulators="f64 (energy, Q, sum n)",
                   parallelism=("replicas split across %d GPUs" % args.gpus if args.shard and args.gpus > 1
                                else "independent replicas x%d" % max(1, args.gpus)))
@@ -726,7 +766,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return 0
-        r, why = reference_cpu(args.steps, args.warmup)
+        r, why = reference_cpu(args.steps, args.warmup, name=args.workload)
         if r is None:
             print(json.dumps({"impl": "reference", "unavailable": why}))
             return 0
@@ -737,10 +777,7 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic", "config": config,
                 "cpu_baseline": {"value": v, "unit": "site-updates/s", "cores": r["threads"], "kind": "reference",
-                                 "sample": "%d measured sweeps of the 256^3 lattice after %d warm-up sweeps, from the "
-                                           "GPU arm's initial directors (reference EvolveN::Monte_Carlo_Step + "
-                                           "energy_calculator + Q_tensor + eigen, GSL replaced by the shim)"
-                                           % (r["steps"], r["warmup"])},
+                                 "sample": reference_sample(r, args.workload)},
                 "e2e": {"value": v, "unit": "site-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return 0
@@ -750,13 +787,11 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     res = gpu_arm(args, rank, world, local_rank)
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "c2":
-        r, why = reference_cpu(10, 1, budget_s=25.0)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r, why = reference_cpu(10, 1, budget_s=25.0, name=args.workload)
         if r is not None:
             cpu = {"value": r["sites"] * r["steps"] / r["seconds"], "unit": "site-updates/s", "cores": r["threads"],
-                   "kind": "reference",
-                   "sample": "%d measured sweeps of the same 256^3 lattice (the GPU arm's initial directors) after 1 "
-                             "warm-up sweep, reference OpenMP CPU code (oracle/_ref, GSL shim)" % r["steps"]}
+                   "kind": "reference", "sample": reference_sample(r, args.workload)}
         else:
             cpu = {"value": None, "unavailable": why}
     if world > 1:

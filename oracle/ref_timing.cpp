@@ -10,7 +10,8 @@
 // arm of bench.py passes its own initial state this way, so both arms start from the same directors.
 // One step = EvolveN::Monte_Carlo_Step (src/evolve.cpp:85-221) and, with measure = 1, the measurement the
 // reference's mode loops do after each measurement sweep: energy_calculator + Q_tensor +
-// Eigen_value_evaluation (src/evolve_thermal.cpp:95-102). Prints one JSON line with the wall time of the timed
+// Eigen_value_evaluation (src/evolve_thermal.cpp:95-102). The steps run at T = Ti and, in the electric mode, at the
+// field Ei (one scan point of any mode). Prints one JSON line with the wall time of the timed
 // steps, the thread count (OMP_NUM_THREADS or all cores) and the site count.
 #include <math.h>
 #include <omp.h>
@@ -112,6 +113,9 @@ int main(int argc, char **argv) {
     ev->geometry->bulk_potential = &Bulk_Energy_Selinger_Pear;
   }
   params.T = params.Ti;
+  // the electric mode's first scan point (src/evolve_electric.cpp:67: elecE = Ei at the first field value); the
+  // other modes keep elecE = 1
+  if (strcasecmp(params.evol, "electric") == 0) params.elecE = params.elecEi;
 
   const int threads = omp_get_max_threads();
   gsl_rng **rng = (gsl_rng **)calloc(threads, sizeof(gsl_rng *));
