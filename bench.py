@@ -299,10 +299,17 @@ def reference_sample(r, name):
             % (r["steps"], which, r["warmup"]))
 
 
-def program_runs(exe, k_meas, k_therm, k0=200, repeats=2):
+def c2_program_text(mct, mcs):
+    """C2's input for the reference's program in its GPU thermal mode, with mct thermalisation and mcs measured
+    sweeps."""
+    text = c2_input_text().replace("evol thermal", "evol thermalGPU")
+    return text.replace("MCT 200", "MCT %d" % mct).replace("MCS 1000", "MCS %d" % mcs)
+
+
+def program_runs(exe, k_meas, k_therm, k0=200, repeats=2, text_for=c2_program_text, sites=256 ** 3):
     """The reference's differencing method on a whole program (paper/benchmark: the fastest of the repetitions of a
-    run with more sweeps minus the fastest of a run with fewer): thermalGPU runs of the 256^3 GHRL slab input, all
-    with at least k0 thermalisation sweeps, with 1 + k_meas and with 1 measured sweep, and with k0 + k_therm
+    run with more sweeps minus the fastest of a run with fewer): GPU-mode runs of one input (text_for(MCT, MCS);
+    the 256^3 GHRL slab by default), all with at least k0 thermalisation sweeps, with 1 + k_meas and with 1 measured sweep, and with k0 + k_therm
     thermalisation sweeps. The k0 sweeps give every run the same kind of final field: the snapshot writer
     (src/io.cpp:59-89, a %g line and a local order parameter per site) takes seconds longer on a thermalised field
     than on the homogeneous start, which a base run of one sweep would still be close to. Every run writes ic.csv
@@ -319,10 +326,8 @@ def program_runs(exe, k_meas, k_therm, k0=200, repeats=2):
         for _ in range(repeats):
             d = tempfile.mkdtemp(prefix="mcl_prog_", dir=where)
             try:
-                text = c2_input_text().replace("evol thermal", "evol thermalGPU")
-                text = text.replace("MCT 200", "MCT %d" % mct).replace("MCS 1000", "MCS %d" % mcs)
                 with open(os.path.join(d, "input.txt"), "w") as f:
-                    f.write(text)
+                    f.write(text_for(mct, mcs))
                 t0 = time.perf_counter()
                 p = subprocess.run([exe, "input.txt"], cwd=d, capture_output=True, text=True, timeout=1200,
                                    env=dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count() or 1)))
@@ -337,7 +342,6 @@ def program_runs(exe, k_meas, k_therm, k0=200, repeats=2):
     base = run(k0, 1)
     meas = run(k0, 1 + k_meas)
     therm = run(k0 + k_therm, 1)
-    sites = 256 ** 3
     return {"measured_s_per_sweep": (meas - base) / k_meas, "thermalisation_s_per_sweep": (therm - base) / k_therm,
             "sites": sites, "steps": k_meas, "thermalisation_sweeps": k_therm, "base_thermalisation_sweeps": k0,
             "runs_s": [base, meas, therm], "repeats": repeats, "run_dir": where or "default temporary directory"}
@@ -361,17 +365,45 @@ def dropin(steps):
     return program_runs(exe, max(steps, 20000), max(steps, 20000)), None
 
 
-def reference_gpu(steps, variant):
+# Sweeps per difference of the reference GPU program, by workload: (measured, thermalisation). Each difference
+# must stand well above the run-to-run noise of one program run (its set-up and its ic.csv and snapshot files).
+REFERENCE_GPU_SWEEPS = {"c1": (2000, 20000), "c2": (20, 1000), "c4": (40, 4000)}
+
+
+def reference_gpu(steps, variant, name="c2"):
     """Context, not the reference arm: the reference's own GPU program (its .cu path, oracle/_ref/mclics_ref_gpu
-    built for sm_100, or mclics_ref_gpu_jit as shipped, PTX compiled by the driver) on the 256^3 GHRL slab, timed by
-    the reference's own differencing (paper/benchmark: a run with more sweeps minus a run with fewer). Measured
-    sweeps (thermalGPU's MCS loop: sweep, energy, lattice copied to the host, Q tensor and S there) and
-    thermalisation sweeps (MCT: the eight sublattice launches and the acceptance reduction only) separately. The
-    reference has no noisy initial condition, so it starts from (0, 0, 1)."""
+    built for sm_100, or mclics_ref_gpu_jit as shipped, PTX compiled by the driver), timed by the reference's own
+    differencing (paper/benchmark: a run with more sweeps minus a run with fewer). Measured sweeps (the GPU thermal
+    mode's MCS loop: sweep, energy, lattice copied to the host, Q tensor and S there) and thermalisation sweeps (MCT:
+    the eight sublattice launches and the acceptance reduction only) separately. One program is one lattice, so a
+    workload of several replicas is one program per replica, their per-sweep times added. On C2 the reference has
+    no noisy initial condition, so it starts from (0, 0, 1); the others start from its own random directors. C3 and
+    C5 (64 and 32 programs, three runs each, twice) are not timed."""
     exe = os.path.join(ROOT, "oracle", "_ref", "mclics_ref_gpu" if variant == "sm_100" else "mclics_ref_gpu_jit")
     if not os.path.exists(exe):
         return None, "%s not built (make -C oracle REF=... refgpu)" % os.path.relpath(exe, ROOT)
-    return program_runs(exe, steps, max(steps, 1000)), None
+    if name not in REFERENCE_GPU_SWEEPS:
+        return None, "not timed for workload %s: one reference program per replica (%s)" % (
+            name, "64 programs" if name == "c3" else "32 programs")
+    if name == "c2":
+        return program_runs(exe, steps, max(steps, 1000)), None
+    k_meas, k_therm = REFERENCE_GPU_SWEEPS[name]
+    _, reps, _, _ = workload(name)
+    parts = []
+    for rep in reps:
+        base_text = reference_input_text(name, rep).replace("evol thermal", "evol thermalGPU")
+
+        def text_for(mct, mcs, base_text=base_text):
+            return base_text.replace("MCT 0", "MCT %d" % mct).replace("MCS 1", "MCS %d" % mcs)
+
+        parts.append(program_runs(exe, max(steps, k_meas), k_therm, k0=200, text_for=text_for,
+                                  sites=rep["nx"] * rep["ny"] * rep["nz"]))
+    r = dict(parts[0])
+    r["sites"] = sum(x["sites"] for x in parts)
+    r["measured_s_per_sweep"] = sum(x["measured_s_per_sweep"] for x in parts)
+    r["thermalisation_s_per_sweep"] = sum(x["thermalisation_s_per_sweep"] for x in parts)
+    r["runs_s"] = [x["runs_s"] for x in parts] if len(parts) > 1 else parts[0]["runs_s"]
+    return r, None
 
 
 def gpu_arm(args, rank, world, local_rank):
@@ -726,8 +758,8 @@ def main():
         return learned_compare(args)
     if args.zslab and args.impl != "reference":
         return zslab_main(args, rank, world, local_rank)
-    # the reference arm runs every workload; the whole-program arms (dropin, reference-gpu) run C2's input only
-    _, _, config, _ = workload(args.workload if args.impl in ("mclics_b200", "reference") else "c2")
+    # the reference arms run the chosen workload; the drop-in's whole-program timing runs C2's input only
+    _, _, config, _ = workload(args.workload if args.impl in ("mclics_b200", "reference", "reference-gpu") else "c2")
     config = dict(config, step="1 sweep + measurement of every lattice", accumulators="f64 (energy, Q, sum n)",
                   parallelism=("replicas split across %d GPUs" % args.gpus if args.shard and args.gpus > 1
                                else "independent replicas x%d" % max(1, args.gpus)))
@@ -750,7 +782,7 @@ def main():
     if args.impl == "reference-gpu":  # context only: the driver's reference arm is the CPU path above
         if rank != 0:
             return 0
-        r, why = reference_gpu(args.steps, args.reference_gpu_build)
+        r, why = reference_gpu(args.steps, args.reference_gpu_build, args.workload)
         if r is None:
             print(json.dumps({"impl": "reference-gpu", "unavailable": why}))
             return 0
@@ -758,7 +790,8 @@ def main():
         print(json.dumps({"impl": "reference-gpu", "build": args.reference_gpu_build, "metric": METRIC, "value": v,
                           "unit": "site-updates/s", "n_gpus": 1, "steps": r["steps"],
                           "ms_per_step": 1e3 * r["measured_s_per_sweep"], "higher_is_better": True,
-                          "config": dict(config, start="(0, 0, 1): the reference has no noisy initial condition"),
+                          "config": dict(config, start="(0, 0, 1): the reference has no noisy initial condition"
+                                         if args.workload == "c2" else "the reference program's own random directors"),
                           "thermalisation_sweeps_per_s_site_updates": r["sites"] / r["thermalisation_s_per_sweep"],
                           **program_method(r)}))
         return 0

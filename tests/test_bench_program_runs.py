@@ -18,7 +18,7 @@ import os, sys, time
 kv = dict(line.split()[:2] for line in open(sys.argv[1]) if len(line.split()) >= 2)
 mct, mcs = int(kv["MCT"]), int(kv["MCS"])
 with open(os.environ["FAKE_PROGRAM_LOG"], "a") as f:
-    f.write("%s %d %d\\n" % (kv["evol"], mct, mcs))
+    f.write("%s %d %d %s %s\\n" % (kv["evol"], mct, mcs, kv.get("Ti", "-"), kv["Nx"]))
 if os.environ.get("FAKE_PROGRAM_FAIL"):
     sys.stderr.write("simulated failure\\n")
     sys.exit(3)
@@ -57,3 +57,24 @@ def test_a_failing_program_is_reported(fake_program, monkeypatch):
     monkeypatch.setenv("FAKE_PROGRAM_FAIL", "1")
     with pytest.raises(RuntimeError, match="simulated failure"):
         bench.program_runs(exe, k_meas=1, k_therm=1, k0=1, repeats=1)
+
+
+def test_reference_gpu_program_runs_one_program_per_replica(fake_program, tmp_path, monkeypatch):
+    """--impl reference-gpu on C4: three programs (one per temperature), each differenced as above; C3 and C5 are
+    reported as not timed."""
+    exe, log = fake_program
+    root = tmp_path / "root"
+    (root / "oracle" / "_ref").mkdir(parents=True)
+    os.symlink(exe, root / "oracle" / "_ref" / "mclics_ref_gpu")
+    monkeypatch.setattr(bench, "ROOT", str(root))
+    monkeypatch.setattr(bench, "REFERENCE_GPU_SWEEPS", dict(bench.REFERENCE_GPU_SWEEPS, c4=(10, 20)))
+    r, why = bench.reference_gpu(1, "sm_100", "c4")
+    assert why is None
+    runs = [line.split() for line in log.read_text().splitlines()]
+    assert len(runs) == 3 * 6 and all(x[0] == "thermalGPU" and x[4] == "128" for x in runs)
+    assert sorted({float(x[3]) for x in runs}) == [0.3, 0.8, 1.12]
+    assert [(int(x[1]), int(x[2])) for x in runs[:6]] == [(200, 1)] * 2 + [(200, 11)] * 2 + [(220, 1)] * 2
+    assert r["sites"] == 3 * 128 ** 3 and len(r["runs_s"]) == 3
+    for name in ("c3", "c5"):
+        r, why = bench.reference_gpu(1, "sm_100", name)
+        assert r is None and "not timed" in why
