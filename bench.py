@@ -23,10 +23,13 @@ reference's thermalGPU loop. Metric: site updates per second (whole job, all GPU
   roofline   the sweep kernel(s) only: algorithmic 24 B per site update (one FP32 director read + write) per
              sweep / kernel time, against the measured HBM copy bandwidth.
   cpu_baseline  the reference's own OpenMP CPU sweep + measurement (oracle/_ref/mclics_ref_timing, built from the
-             reference sources) on all host cores, on a bounded sample of the same lattice.
+             reference sources) on all host cores, on a bounded sample of the same lattice (of the workload's
+             replicas, for --workload cN).
 
 --impl reference times that reference CPU path alone (rank 0) and prints its line with "impl": "reference"; with
 --workload cN it times that workload's replicas (one after another, from the GPU arm's initial directors).
+--impl reference-gpu and --impl dropin are context lines: the reference's own GPU program, and that program with
+this library behind its GPU modes, timed as whole programs by the reference's differencing method.
 Multi-GPU (torchrun): every rank sweeps its own independent replica of the workload (no data-path collective;
 "scaling": "weak"); value = all ranks' site updates / the slowest rank's device time.
 """
