@@ -297,9 +297,9 @@ def reference_sample(r, name):
              "all %d replicas" % r["replicas"] if r["replicas_timed"] == r["replicas"] and r["replicas"] > 1 else
              "the lattice" if r["replicas"] == 1 else
              "%d of the %d replicas (every %d-th)" % (r["replicas_timed"], r["replicas"], r["replica_stride"]))
-    return ("%d measured sweeps of %s after %d warm-up sweeps, from the GPU arm's initial directors (reference "
+    return ("%d measured sweep%s of %s after %d warm-up sweep%s, from the GPU arm's initial directors (reference "
             "EvolveN::Monte_Carlo_Step + energy_calculator + Q_tensor + eigen, GSL replaced by the shim)"
-            % (r["steps"], which, r["warmup"]))
+            % (r["steps"], "" if r["steps"] == 1 else "s", which, r["warmup"], "" if r["warmup"] == 1 else "s"))
 
 
 def c2_program_text(mct, mcs):
